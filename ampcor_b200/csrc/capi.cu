@@ -1,0 +1,727 @@
+// C ABI and host orchestration of the batched tile correlator.
+//
+// The worker (ampcor_handle) plays the role of ampcor::cuda::correlators::Sequential
+// (lib/libampcor_cuda/correlators/Sequential.h, Sequential.icc): it derives the tile layouts from
+// the constructor arguments, owns the host arena of the pair-by-pair API and runs the pipeline.
+// Unlike the reference it allocates its device memory once and reuses it, runs the stages on its
+// own stream with no synchronisation between them, and returns status codes instead of
+// throwing.
+#include "../../include/ampcor_b200.h"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace ampcor_b200;
+
+namespace {
+
+const char* kVersion = "ampcor_b200 0.1.0 (sm_100a)";
+const char* kCopyright =
+    "ampcor_b200: B200-native batched tile correlator with the worker interface of "
+    "isce-framework/ampcor";
+
+std::mutex g_create_mutex;
+std::string g_create_error;
+
+constexpr int kCompiledNV[] = {9, 16, 17, 32, 33};
+
+int round_nv(int w)
+{
+    for (int nv : kCompiledNV)
+        if (nv >= w) return nv;
+    return -1;
+}
+
+int odd_at_least(int x) { return (x % 2) ? x : x + 1; }
+int round4(int x) { return (x + 3) & ~3; }
+
+// split of one correlation surface over the warps of a CTA and its shared-memory layout;
+// extra_win / extra_chip reserve room for the zoom stage of the fine kernel
+bool plan_ncc(int R, int W, int extra_win, int extra_chip, NccGeom& g, std::string& err)
+{
+    std::memset(&g, 0, sizeof(g));
+    const int C = W - R + 1;
+    if (R < 2 || C < 1) {
+        err = "chip must be at least 2x2 and no larger than the search window";
+        return false;
+    }
+    g.R = R;
+    g.W = W;
+    g.C = C;
+    // column blocks: a first block of up to 33 placements, then blocks of 32
+    const int blocks = (C <= 33) ? 1 : 1 + (C - 33 + 31) / 32;
+    if (blocks > kMaxVB) {
+        err = "search margin too large for this build (at most 8 column blocks)";
+        return false;
+    }
+    g.n_vb = blocks;
+    int v0 = 0;
+    int need_s = W, need_cs = R;
+    for (int b = 0; b < blocks; ++b) {
+        const int w = (b == 0) ? C - 32 * (blocks - 1) : 32;
+        const int nv = round_nv(w);
+        if (nv < 0) {
+            err = "internal: no register block for width " + std::to_string(w);
+            return false;
+        }
+        const int steps = (R + nv - 1) / nv;
+        g.vb_v0[b] = v0;
+        g.vb_w[b] = w;
+        g.vb_nv[b] = nv;
+        g.vb_steps[b] = steps;
+        need_s = std::max(need_s, v0 + steps * nv + nv);
+        need_cs = std::max(need_cs, steps * nv);
+        v0 += w;
+    }
+    g.S = odd_at_least(need_s);
+    g.CS = odd_at_least(need_cs);
+    g.n_ub = C / 32;
+    if (g.n_ub * g.n_vb > kWarps) {
+        err = "search margin too large for this build (placement blocks exceed the warps)";
+        return false;
+    }
+    g.n_kc = g.n_ub ? std::min(R, std::max(1, kWarps / (g.n_ub * g.n_vb))) : 0;
+    g.n_main = g.n_ub * g.n_vb * g.n_kc;
+    g.n_tkc = (R + 31) / 32;
+    g.n_trans = (C - 32 * g.n_ub) * g.n_vb * g.n_tkc;
+
+    const int win_f = std::max({W * g.S, g.n_main * 32 * kSlot, extra_win});
+    const int chip_f = std::max({R * g.CS, 4 * kStatRows * (W + 1), extra_chip});
+    int off = 0;
+    g.off_win = off;
+    off += round4(win_f);
+    g.off_chip = off;
+    off += round4(chip_f);
+    g.off_inv = off;
+    off += round4(C * C);
+    g.off_gam = off;
+    off += round4(C * C);
+    g.off_trans = off;
+    off += round4(std::max(1, g.n_trans) * kSlot);
+    g.off_red = off;
+    off += 128;
+    g.off_aux = off;
+    g.smem_bytes = off * 4;
+    if (g.smem_bytes > 227 * 1024) {
+        err = "tile geometry needs " + std::to_string(g.smem_bytes) +
+              " bytes of shared memory; this build supports at most 232448";
+        return false;
+    }
+    return true;
+}
+
+bool plan_interp(int N, int f, InterpGeom& ig, std::string& err)
+{
+    std::memset(&ig, 0, sizeof(ig));
+    if (N % kQB) {
+        err = "refinement tiles must be a multiple of 8 pixels (chip and chip + 2 * refine margin)";
+        return false;
+    }
+    ig.N = N;
+    ig.f = f;
+    ig.F = f * N;
+    ig.NS = odd_at_least(N);
+    ig.YS = odd_at_least(ig.F);
+    ig.taps_len = 2 * N + 2 * kQB;
+    int off = 0;
+    ig.off_x = off;
+    off += round4(2 * N * ig.NS);
+    ig.off_y = off;
+    off += round4(2 * N * ig.YS);
+    ig.off_taps = off;
+    off += round4(std::max(1, f - 1) * ig.taps_len);
+    ig.smem_bytes = off * 4;
+    if (ig.smem_bytes > 227 * 1024) {
+        err = "refinement tile too large for shared memory in this build";
+        return false;
+    }
+    return true;
+}
+
+// band-limited interpolation kernel of an N-periodic sequence (Nyquist pair halved for even N):
+// the zero-padded inverse FFT with a 1/N scale, written as a sum of cosines
+double dirichlet(int N, double d)
+{
+    double s = 1.0;
+    if (N % 2) {
+        for (int n = 1; n <= (N - 1) / 2; ++n) s += 2.0 * std::cos(2.0 * M_PI * n * d / N);
+    } else {
+        for (int n = 1; n < N / 2; ++n) s += 2.0 * std::cos(2.0 * M_PI * n * d / N);
+        s += std::cos(M_PI * d);
+    }
+    return s / N;
+}
+
+// taps[s][d] = D_N(d - (N-1) + s/f) for phases s in [s0, f)
+std::vector<float> taps_table(int N, int f, int s0, int len)
+{
+    std::vector<float> t((size_t)(f - s0) * len);
+    for (int s = s0; s < f; ++s)
+        for (int d = 0; d < len; ++d)
+            t[(size_t)(s - s0) * len + d] = (float)dirichlet(N, d - (N - 1) + (double)s / f);
+    return t;
+}
+
+}  // namespace
+
+struct ampcor_handle {
+    ampcor_params prm{};
+    int R = 0, W = 0, C = 0, M = 0, E = 0, f = 0, m = 0, z = 0, Rf = 0, Wf = 0, Cf = 0, Z = 0;
+    NccGeom gc{}, gf{};
+    InterpGeom ic{}, iw{};
+    ZoomGeom zg{};
+    int refine_smem = 0;
+    cudaStream_t stream = nullptr;
+    float* d_chip_taps = nullptr;
+    float* d_win_taps = nullptr;
+    float* d_zoom_taps = nullptr;
+    // arena API
+    float2* h_arena = nullptr;
+    float2* d_arena = nullptr;
+    float* h_offsets = nullptr;
+    // per-pair buffers
+    size_t cap = 0;
+    long long* d_ref_off = nullptr;
+    long long* d_tgt_off = nullptr;
+    CoarseOut* d_coarse = nullptr;
+    float* d_coarse_peak = nullptr;
+    float2* d_offsets = nullptr;
+    PairDiag* d_diag = nullptr;
+    unsigned int* d_bad = nullptr;
+    // refined amplitudes of one chunk of pairs
+    float* d_refined = nullptr;
+    size_t chunk = 0;
+    long long refined_stride = 0;
+    // host-path staging
+    void* d_ref_raster = nullptr;
+    void* d_tgt_raster = nullptr;
+    size_t raster_bytes_ref = 0, raster_bytes_tgt = 0;
+    int32_t* d_ulhc = nullptr;
+    size_t ulhc_cap = 0;
+    float* d_job_offsets = nullptr;
+    size_t job_offsets_cap = 0;
+    ampcor_pair_diag* d_job_diag = nullptr;
+    size_t job_diag_cap = 0;
+    // per-stage timing: (start, stop) event pairs of each kernel launch, per stage
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks[3];
+    std::string err;
+};
+
+namespace {
+
+int fail(ampcor_handle* h, int code, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(ampcor_handle* h, cudaError_t e, const char* what)
+{
+    return fail(h, AMPCOR_E_CUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" +
+                                      cudaGetErrorString(e) + ")");
+}
+
+#define CK(h, call, what)                                  \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
+    } while (0)
+
+template <typename T>
+int grow(ampcor_handle* h, T*& ptr, size_t& cap, size_t n, const char* what)
+{
+    if (cap >= n && ptr) return AMPCOR_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)&ptr, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return fail(h, AMPCOR_E_NOMEM, std::string("allocating ") + what + ": " + cudaGetErrorName(e));
+    }
+    cap = n;
+    return AMPCOR_OK;
+}
+
+int ensure_pairs(ampcor_handle* h, size_t pairs)
+{
+    if (h->cap >= pairs && h->d_ref_off) return AMPCOR_OK;
+    cudaFree(h->d_ref_off);
+    cudaFree(h->d_tgt_off);
+    cudaFree(h->d_coarse);
+    cudaFree(h->d_coarse_peak);
+    cudaFree(h->d_offsets);
+    cudaFree(h->d_diag);
+    h->d_ref_off = h->d_tgt_off = nullptr;
+    h->d_coarse = nullptr;
+    h->d_coarse_peak = nullptr;
+    h->d_offsets = nullptr;
+    h->d_diag = nullptr;
+    h->cap = 0;
+    const size_t n = std::max<size_t>(pairs, 1);
+    if (cudaMalloc(&h->d_ref_off, n * sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&h->d_tgt_off, n * sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&h->d_coarse, n * sizeof(CoarseOut)) != cudaSuccess ||
+        cudaMalloc(&h->d_coarse_peak, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->d_offsets, n * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->d_diag, n * sizeof(PairDiag)) != cudaSuccess)
+        return fail(h, AMPCOR_E_NOMEM, "allocating per-pair device buffers");
+    h->cap = n;
+    return AMPCOR_OK;
+}
+
+// the chunk of pairs whose refined amplitudes are resident at once: a few waves of CTAs,
+// small enough that the refined tiles mostly stay in L2 between the refine and fine kernels
+size_t default_chunk()
+{
+    const char* env = std::getenv("AMPCOR_CHUNK");
+    if (env) {
+        long v = std::strtol(env, nullptr, 10);
+        if (v > 0) return (size_t)v;
+    }
+    return 148 * 4;
+}
+
+int ensure_refined(ampcor_handle* h)
+{
+    if (h->d_refined) return AMPCOR_OK;
+    h->chunk = default_chunk();
+    h->refined_stride = (long long)h->Rf * h->Rf + (long long)h->Wf * h->Wf;
+    cudaError_t e = cudaMalloc(&h->d_refined, h->chunk * h->refined_stride * sizeof(float));
+    if (e != cudaSuccess) {
+        h->d_refined = nullptr;
+        return fail(h, AMPCOR_E_NOMEM, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
+    }
+    return AMPCOR_OK;
+}
+
+// record an event (profiling only); returns nullptr when profiling is off
+cudaEvent_t mark(ampcor_handle* h, cudaStream_t st)
+{
+    if (!h->profiling) return nullptr;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    cudaEventRecord(e, st);
+    return e;
+}
+
+void keep(ampcor_handle* h, int stage, cudaEvent_t a, cudaEvent_t b)
+{
+    if (a && b) h->marks[stage].emplace_back(a, b);
+}
+
+// enqueue coarse -> (refine -> fine) per chunk on stream st
+int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+{
+    if (pairs == 0) return AMPCOR_OK;
+    int rc = ensure_refined(h);
+    if (rc) return rc;
+    cudaEvent_t a = mark(h, st);
+    coarse_kernel<<<(unsigned)pairs, kThreads, h->gc.smem_bytes, st>>>(
+        src, 0, pairs, h->gc, h->m, h->d_coarse, h->d_coarse_peak, coarse_surfaces);
+    CK(h, cudaGetLastError(), "launching the coarse correlation kernel");
+    keep(h, 0, a, mark(h, st));
+    for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
+        const long long n = std::min<long long>((long long)h->chunk, pairs - c0);
+        a = mark(h, st);
+        refine_kernel<<<(unsigned)n, kThreads, h->refine_smem, st>>>(
+            src, c0, n, h->d_coarse, h->ic, h->iw, h->d_chip_taps, h->d_win_taps, h->d_refined,
+            h->refined_stride);
+        CK(h, cudaGetLastError(), "launching the refinement kernel");
+        cudaEvent_t b = mark(h, st);
+        keep(h, 1, a, b);
+        fine_kernel<<<(unsigned)n, kThreads, h->gf.smem_bytes, st>>>(
+            h->d_refined, h->refined_stride, c0, n, src.ref_off, h->gf, h->zg, h->d_zoom_taps,
+            h->d_coarse, h->d_coarse_peak, h->M, h->f, h->m,
+            (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0, offsets, diag, refined_surfaces);
+        CK(h, cudaGetLastError(), "launching the fine correlation kernel");
+        // the fine stage starts at the event that ends the refine stage
+        keep(h, 2, b, mark(h, st));
+    }
+    return AMPCOR_OK;
+}
+
+void drop_marks(ampcor_handle* h)
+{
+    std::vector<cudaEvent_t> seen;
+    for (auto& v : h->marks) {
+        for (auto& pr : v) {
+            for (cudaEvent_t e : {pr.first, pr.second})
+                if (std::find(seen.begin(), seen.end(), e) == seen.end()) seen.push_back(e);
+        }
+        v.clear();
+    }
+    for (cudaEvent_t e : seen) cudaEventDestroy(e);
+}
+
+cudaStream_t pick(ampcor_handle* h, void* stream)
+{
+    return stream ? (cudaStream_t)stream : h->stream;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ampcor_create(const ampcor_params* p, ampcor_handle** out)
+{
+    auto create_fail = [&](int code, const std::string& msg) {
+        std::lock_guard<std::mutex> lk(g_create_mutex);
+        g_create_error = msg;
+        return code;
+    };
+    if (!p || !out) return create_fail(AMPCOR_E_ARG, "null argument");
+    *out = nullptr;
+    if (p->ref_lines != p->ref_samples || p->tgt_lines != p->tgt_samples)
+        return create_fail(AMPCOR_E_SHAPE, "chips and search windows must be square");
+    if (p->tgt_lines < p->ref_lines || (p->tgt_lines - p->ref_lines) % 2)
+        return create_fail(AMPCOR_E_SHAPE, "window must exceed the chip by an even margin");
+    if (p->refine_factor < 1 || p->zoom_factor < 1)
+        return create_fail(AMPCOR_E_ARG, "refine and zoom factors must be positive");
+    if (p->ref_lines > 4096 || p->refine_factor > 16 || p->zoom_factor > 64 ||
+        p->refine_margin > 1024)
+        return create_fail(AMPCOR_E_SHAPE, "geometry out of range");
+
+    ampcor_handle* h = new (std::nothrow) ampcor_handle();
+    if (!h) return create_fail(AMPCOR_E_NOMEM, "allocating the worker");
+    h->prm = *p;
+    h->R = (int)p->ref_lines;
+    h->W = (int)p->tgt_lines;
+    h->C = h->W - h->R + 1;
+    h->M = (h->W - h->R) / 2;
+    h->f = (int)p->refine_factor;
+    h->m = (int)p->refine_margin;
+    h->z = (int)p->zoom_factor;
+    h->E = h->R + 2 * h->m;
+    h->Rf = h->f * h->R;
+    h->Wf = h->f * h->E;
+    h->Cf = 2 * h->f * h->m + 1;
+    h->Z = h->z * h->Cf;
+    std::string err;
+    if (h->E > h->W) {
+        delete h;
+        return create_fail(AMPCOR_E_SHAPE, "refinement neighbourhood (chip + 2 * refine margin) exceeds the window");
+    }
+    // zoom stage sizes (taps of z phases, the row-interpolated surface Cf x Z)
+    h->zg.Cf = h->Cf;
+    h->zg.z = h->z;
+    h->zg.Z = h->Z;
+    h->zg.cb = 1;
+    for (int cb : {17, 13, 11, 5, 3})
+        if (h->Cf % cb == 0) {
+            h->zg.cb = cb;
+            break;
+        }
+    h->zg.taps_len = 2 * h->Cf + 32;
+    if (!plan_ncc(h->R, h->W, 0, 0, h->gc, err) ||
+        !plan_ncc(h->Rf, h->Wf, h->Cf * h->Z, h->z * h->zg.taps_len, h->gf, err) ||
+        !plan_interp(h->R, h->f, h->ic, err) || !plan_interp(h->E, h->f, h->iw, err)) {
+        delete h;
+        return create_fail(AMPCOR_E_SHAPE, err);
+    }
+    h->refine_smem = std::max(h->ic.smem_bytes, h->iw.smem_bytes);
+
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) {
+        delete h;
+        return create_fail(AMPCOR_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorName(e));
+    }
+    auto cuda_create_fail = [&](cudaError_t ce, const char* what) {
+        ampcor_destroy(h);
+        return create_fail(AMPCOR_E_CUDA, std::string(what) + ": " + cudaGetErrorName(ce));
+    };
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_create_fail(e, "creating the worker stream");
+    if ((e = cudaFuncSetAttribute(coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  h->gc.smem_bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  h->gf.smem_bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  h->refine_smem)) != cudaSuccess)
+        return cuda_create_fail(e, "configuring kernel shared memory");
+
+    const std::vector<float> ct = taps_table(h->R, h->f, 1, h->ic.taps_len);
+    const std::vector<float> wt = taps_table(h->E, h->f, 1, h->iw.taps_len);
+    const std::vector<float> zt = taps_table(h->Cf, h->z, 0, h->zg.taps_len);
+    auto upload = [&](float*& d, const std::vector<float>& v) {
+        cudaError_t ue = cudaMalloc(&d, std::max<size_t>(v.size(), 1) * sizeof(float));
+        if (ue != cudaSuccess) return ue;
+        if (!v.empty()) ue = cudaMemcpy(d, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice);
+        return ue;
+    };
+    if ((e = upload(h->d_chip_taps, ct)) != cudaSuccess || (e = upload(h->d_win_taps, wt)) != cudaSuccess ||
+        (e = upload(h->d_zoom_taps, zt)) != cudaSuccess)
+        return cuda_create_fail(e, "uploading interpolation taps");
+    if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess)
+        return cuda_create_fail(e, "allocating the bounds counter");
+    *out = h;
+    return AMPCOR_OK;
+}
+
+int ampcor_destroy(ampcor_handle* h)
+{
+    if (!h) return AMPCOR_E_ARG;
+    cudaSetDevice(h->prm.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_chip_taps);
+    cudaFree(h->d_win_taps);
+    cudaFree(h->d_zoom_taps);
+    cudaFree(h->d_arena);
+    cudaFree(h->d_ref_off);
+    cudaFree(h->d_tgt_off);
+    cudaFree(h->d_coarse);
+    cudaFree(h->d_coarse_peak);
+    cudaFree(h->d_offsets);
+    cudaFree(h->d_diag);
+    cudaFree(h->d_bad);
+    cudaFree(h->d_refined);
+    cudaFree(h->d_ref_raster);
+    cudaFree(h->d_tgt_raster);
+    cudaFree(h->d_ulhc);
+    cudaFree(h->d_job_offsets);
+    cudaFree(h->d_job_diag);
+    drop_marks(h);
+    if (h->h_arena) cudaFreeHost(h->h_arena);
+    if (h->h_offsets) cudaFreeHost(h->h_offsets);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return AMPCOR_OK;
+}
+
+static int ensure_arena(ampcor_handle* h)
+{
+    if (h->h_arena) return AMPCOR_OK;
+    const size_t pixels = h->prm.pairs * ((size_t)h->R * h->R + (size_t)h->W * h->W);
+    cudaError_t e = cudaMallocHost(&h->h_arena, std::max<size_t>(pixels, 1) * sizeof(float2));
+    if (e != cudaSuccess) {
+        h->h_arena = nullptr;
+        return fail(h, AMPCOR_E_NOMEM, "allocating the host tile arena");
+    }
+    std::memset(h->h_arena, 0, pixels * sizeof(float2));
+    return AMPCOR_OK;
+}
+
+static int add_tile(ampcor_handle* h, uint64_t pid, const void* tile, uint64_t row_stride, bool ref)
+{
+    if (!h) return AMPCOR_E_ARG;
+    if (!tile) return fail(h, AMPCOR_E_ARG, "null tile");
+    if (pid >= h->prm.pairs) return fail(h, AMPCOR_E_ARG, "pair id out of range");
+    const int dim = ref ? h->R : h->W;
+    if (row_stride < (uint64_t)dim) return fail(h, AMPCOR_E_ARG, "row stride smaller than the tile");
+    int rc = ensure_arena(h);
+    if (rc) return rc;
+    const size_t cells = (size_t)h->R * h->R + (size_t)h->W * h->W;
+    float2* dst = h->h_arena + pid * cells + (ref ? 0 : (size_t)h->R * h->R);
+    const float2* src = static_cast<const float2*>(tile);
+    for (int r = 0; r < dim; ++r) std::memcpy(dst + (size_t)r * dim, src + r * row_stride, dim * sizeof(float2));
+    return AMPCOR_OK;
+}
+
+int ampcor_add_reference(ampcor_handle* h, uint64_t pid, const void* tile, uint64_t row_stride)
+{
+    return add_tile(h, pid, tile, row_stride, true);
+}
+
+int ampcor_add_target(ampcor_handle* h, uint64_t pid, const void* tile, uint64_t row_stride)
+{
+    return add_tile(h, pid, tile, row_stride, false);
+}
+
+int ampcor_adjust(ampcor_handle* h, const float** offsets)
+{
+    if (!h || !offsets) return fail(h, AMPCOR_E_ARG, "null argument");
+    *offsets = nullptr;
+    const size_t P = h->prm.pairs;
+    int rc = ensure_arena(h);
+    if (rc) return rc;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    const size_t cells = (size_t)h->R * h->R + (size_t)h->W * h->W;
+    if (!h->d_arena) CK(h, cudaMalloc(&h->d_arena, std::max<size_t>(P * cells, 1) * sizeof(float2)), "allocating the device arena");
+    if (!h->h_offsets) CK(h, cudaMallocHost(&h->h_offsets, std::max<size_t>(2 * P, 1) * sizeof(float)), "allocating the offset field");
+    if ((rc = ensure_pairs(h, P))) return rc;
+    cudaStream_t st = h->stream;
+    if (P) {
+        CK(h, cudaMemcpyAsync(h->d_arena, h->h_arena, P * cells * sizeof(float2), cudaMemcpyHostToDevice, st),
+           "pushing the tile arena");
+        arena_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
+            (long long)P, (long long)h->R * h->R, (long long)h->W * h->W, h->d_ref_off, h->d_tgt_off);
+        CK(h, cudaGetLastError(), "launching the arena offsets kernel");
+        PairSource src{h->d_arena, h->d_ref_off, h->R, h->d_arena, h->d_tgt_off, h->W};
+        if ((rc = run_pipeline(h, src, (long long)P, h->d_offsets, h->d_diag, nullptr, nullptr, st))) return rc;
+        CK(h, cudaMemcpyAsync(h->h_offsets, h->d_offsets, 2 * P * sizeof(float), cudaMemcpyDeviceToHost, st),
+           "harvesting the offset field");
+    }
+    CK(h, cudaStreamSynchronize(st), "running the correlation pipeline");
+    *offsets = h->h_offsets;
+    return AMPCOR_OK;
+}
+
+int ampcor_diagnostics(ampcor_handle* h, ampcor_pair_diag* diag)
+{
+    if (!h || !diag) return fail(h, AMPCOR_E_ARG, "null argument");
+    if (!h->d_diag) return fail(h, AMPCOR_E_STATE, "no adjust has run");
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    static_assert(sizeof(ampcor_pair_diag) == sizeof(PairDiag), "diagnostic layout");
+    CK(h, cudaMemcpy(diag, h->d_diag, h->prm.pairs * sizeof(PairDiag), cudaMemcpyDeviceToHost),
+       "copying diagnostics");
+    return AMPCOR_OK;
+}
+
+static int check_job(ampcor_handle* h, const ampcor_job* j)
+{
+    if (!h) return AMPCOR_E_ARG;
+    if (!j) return fail(h, AMPCOR_E_ARG, "null job");
+    if (j->pairs && (!j->ref || !j->tgt || !j->ulhc || !j->offsets))
+        return fail(h, AMPCOR_E_ARG, "null raster, corner or offset pointer");
+    if (j->ref_lines <= 0 || j->ref_samples <= 0 || j->tgt_lines <= 0 || j->tgt_samples <= 0)
+        return fail(h, AMPCOR_E_ARG, "empty raster");
+    if (j->pairs > 0x7fffffffull) return fail(h, AMPCOR_E_ARG, "too many pairs in one batch");
+    return AMPCOR_OK;
+}
+
+int ampcor_correlate(ampcor_handle* h, const ampcor_job* j, void* stream)
+{
+    int rc = check_job(h, j);
+    if (rc) return rc;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    if ((rc = ensure_pairs(h, j->pairs))) return rc;
+    cudaStream_t st = pick(h, stream);
+    if (j->pairs == 0) return AMPCOR_OK;
+    pair_offsets_kernel<<<(unsigned)((j->pairs + 255) / 256), 256, 0, st>>>(
+        j->ulhc, (long long)j->pairs, j->ref_lines, j->ref_samples, j->tgt_lines, j->tgt_samples,
+        h->R, h->W, h->d_ref_off, h->d_tgt_off, h->d_bad);
+    CK(h, cudaGetLastError(), "launching the pair offsets kernel");
+    PairSource src{static_cast<const float2*>(j->ref), h->d_ref_off, j->ref_samples,
+                   static_cast<const float2*>(j->tgt), h->d_tgt_off, j->tgt_samples};
+    return run_pipeline(h, src, (long long)j->pairs, reinterpret_cast<float2*>(j->offsets),
+                        reinterpret_cast<PairDiag*>(j->diag), j->coarse_surfaces,
+                        j->refined_surfaces, st);
+}
+
+int ampcor_synchronize(ampcor_handle* h, void* stream)
+{
+    if (!h) return AMPCOR_E_ARG;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    cudaStream_t st = pick(h, stream);
+    unsigned int bad = 0;
+    CK(h, cudaMemcpyAsync(&bad, h->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, st), "reading the bounds counter");
+    CK(h, cudaStreamSynchronize(st), "running the correlation pipeline");
+    if (bad) {
+        CK(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned int), st), "resetting the bounds counter");
+        CK(h, cudaStreamSynchronize(st), "resetting the bounds counter");
+        return fail(h, AMPCOR_E_BOUNDS, std::to_string(bad) + " tile pair(s) leave their raster; their offsets are NaN");
+    }
+    return AMPCOR_OK;
+}
+
+int ampcor_correlate_host(ampcor_handle* h, const ampcor_job* j)
+{
+    int rc = check_job(h, j);
+    if (rc) return rc;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    if (j->pairs == 0) return AMPCOR_OK;
+    const size_t rb = (size_t)j->ref_lines * j->ref_samples * sizeof(float2);
+    const size_t tb = (size_t)j->tgt_lines * j->tgt_samples * sizeof(float2);
+    if (h->raster_bytes_ref < rb) {
+        cudaFree(h->d_ref_raster);
+        h->d_ref_raster = nullptr;
+        h->raster_bytes_ref = 0;
+        CK(h, cudaMalloc(&h->d_ref_raster, rb), "allocating the reference raster");
+        h->raster_bytes_ref = rb;
+    }
+    if (h->raster_bytes_tgt < tb) {
+        cudaFree(h->d_tgt_raster);
+        h->d_tgt_raster = nullptr;
+        h->raster_bytes_tgt = 0;
+        CK(h, cudaMalloc(&h->d_tgt_raster, tb), "allocating the secondary raster");
+        h->raster_bytes_tgt = tb;
+    }
+    if ((rc = grow(h, h->d_ulhc, h->ulhc_cap, 4 * j->pairs, "pair corners"))) return rc;
+    if ((rc = grow(h, h->d_job_offsets, h->job_offsets_cap, 2 * j->pairs, "offsets"))) return rc;
+    if (j->diag && (rc = grow(h, h->d_job_diag, h->job_diag_cap, j->pairs, "diagnostics"))) return rc;
+    cudaStream_t st = h->stream;
+    CK(h, cudaMemcpyAsync(h->d_ref_raster, j->ref, rb, cudaMemcpyHostToDevice, st), "uploading the reference raster");
+    CK(h, cudaMemcpyAsync(h->d_tgt_raster, j->tgt, tb, cudaMemcpyHostToDevice, st), "uploading the secondary raster");
+    CK(h, cudaMemcpyAsync(h->d_ulhc, j->ulhc, 4 * j->pairs * sizeof(int32_t), cudaMemcpyHostToDevice, st),
+       "uploading the pair corners");
+    ampcor_job dj = *j;
+    dj.ref = h->d_ref_raster;
+    dj.tgt = h->d_tgt_raster;
+    dj.ulhc = h->d_ulhc;
+    dj.offsets = h->d_job_offsets;
+    dj.diag = j->diag ? h->d_job_diag : nullptr;
+    dj.coarse_surfaces = nullptr;
+    dj.refined_surfaces = nullptr;
+    if ((rc = ampcor_correlate(h, &dj, st))) return rc;
+    CK(h, cudaMemcpyAsync(j->offsets, h->d_job_offsets, 2 * j->pairs * sizeof(float), cudaMemcpyDeviceToHost, st),
+       "downloading the offsets");
+    if (j->diag)
+        CK(h, cudaMemcpyAsync(j->diag, h->d_job_diag, j->pairs * sizeof(ampcor_pair_diag), cudaMemcpyDeviceToHost, st),
+           "downloading the diagnostics");
+    return ampcor_synchronize(h, st);
+}
+
+int ampcor_profile(ampcor_handle* h, int enable)
+{
+    if (!h) return AMPCOR_E_ARG;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    drop_marks(h);
+    h->profiling = enable != 0;
+    return AMPCOR_OK;
+}
+
+int ampcor_stage_times(ampcor_handle* h, double* coarse_ms, double* refine_ms, double* fine_ms,
+                       uint64_t* launches)
+{
+    if (!h) return AMPCOR_E_ARG;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    double t[3] = {0.0, 0.0, 0.0};
+    uint64_t n = 0;
+    for (int s = 0; s < 3; ++s)
+        for (auto& pr : h->marks[s]) {
+            CK(h, cudaEventSynchronize(pr.second), "waiting for a stage event");
+            float ms = 0.0f;
+            CK(h, cudaEventElapsedTime(&ms, pr.first, pr.second), "reading a stage event");
+            t[s] += ms;
+            ++n;
+        }
+    drop_marks(h);
+    if (coarse_ms) *coarse_ms = t[0];
+    if (refine_ms) *refine_ms = t[1];
+    if (fine_ms) *fine_ms = t[2];
+    if (launches) *launches = n;
+    return AMPCOR_OK;
+}
+
+int ampcor_surface_dims(const ampcor_handle* h, int32_t* coarse, int32_t* refined, int32_t* zoomed)
+{
+    if (!h) return AMPCOR_E_ARG;
+    if (coarse) *coarse = h->C;
+    if (refined) *refined = h->Cf;
+    if (zoomed) *zoomed = h->Z;
+    return AMPCOR_OK;
+}
+
+const char* ampcor_last_error(const ampcor_handle* h)
+{
+    if (h) return h->err.c_str();
+    std::lock_guard<std::mutex> lk(g_create_mutex);
+    return g_create_error.c_str();
+}
+
+const char* ampcor_version(void) { return kVersion; }
+const char* ampcor_copyright(void) { return kCopyright; }
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// Device-side declarations of the sm_100a batched tile correlator.
+//
+// The pipeline per tile pair (reference: lib/libampcor_cuda/correlators/Sequential.icc:47-141):
+//   coarse_kernel  - gather the chip and search window from the complex64 sources, detect
+//                    (detect.cu:78-115), chip mean/sigma (refStats.cu:118-302), FP64 window box
+//                    statistics (sat.cu:81-149, tgtStats.cu:88-168), NCC over every placement
+//                    (correlate.cu:160-318), first strict maximum (maxcor.cu:79-133) and nudge
+//                    (nudge.cu:81-143), all in one CTA with the tiles resident in shared memory.
+//   refine_kernel  - band-limited upsampling of the complex chip and of the (R+2m)^2
+//                    neighbourhood of the coarse peak (the intent of Sequential.icc:703-1087 and
+//                    migrate.cu:101-154), written out as refined amplitudes.
+//   fine_kernel    - refined NCC, band-limited zoom of the refined surface (intent of
+//                    Sequential.icc:1101-1286), first strict maximum and offset assembly
+//                    (offsets.cu:86-129).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ampcor_b200 {
+
+constexpr int kThreads = 512;            // threads per CTA, one CTA per tile pair
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxVB = 8;                // column blocks of a correlation surface
+constexpr int kSlot = 33;                // row stride of a partial-sum slot (floats)
+constexpr int kStatRows = 8;             // placement rows per window-statistics chunk
+constexpr int kQB = 8;                   // outputs per thread in the interpolation kernels
+
+// how one correlation surface (R x R chip over a W x W window, C = W-R+1 placements per axis)
+// is split over the warps of a CTA, and where each region lives in shared memory
+struct NccGeom {
+    int R, W, C;
+    int S;          // window row stride in shared memory (odd: conflict-free column walks)
+    int CS;         // chip row stride in shared memory (odd)
+    int n_ub;       // full 32-row placement blocks handled lane-per-row ("main" tasks)
+    int n_vb;       // placement column blocks
+    int n_kc;       // chip-row chunks per main task
+    int n_main;     // n_ub * n_vb * n_kc <= kWarps
+    int n_tkc;      // chip-row chunks (32 rows, one per lane) per leftover row
+    int n_trans;    // leftover-row tasks: (C - 32 n_ub) * n_vb * n_tkc
+    int vb_v0[kMaxVB];     // first placement column of the block
+    int vb_w[kMaxVB];      // placement columns in the block
+    int vb_nv[kMaxVB];     // register block width (>= vb_w, one of the compiled widths)
+    int vb_steps[kMaxVB];  // ceil(R / nv): chip columns are zero-padded to steps * nv
+    // shared-memory regions, in floats from the start of the dynamic buffer
+    int off_win, off_part, off_chip, off_inv, off_gam, off_trans, off_red, off_aux;
+    int smem_bytes;
+};
+
+// band-limited interpolation of an N x N complex tile by f (f*N x f*N output)
+struct InterpGeom {
+    int N, f, F;     // F = f N
+    int NS, YS;      // row strides (float2) of the input tile and the row-interpolated tile
+    int taps_len;    // per phase s in [1, f): taps_len entries
+    int off_x, off_y, off_taps;   // shared-memory regions (floats)
+    int smem_bytes;
+};
+
+struct ZoomGeom {
+    int Cf, z, Z;    // refined surface Cf x Cf zoomed to Z x Z, Z = z Cf
+    int cb;          // output rows per thread (Cf % cb == 0)
+    int taps_len;    // per phase s in [0, z)
+};
+
+// per-pair source of the complex64 tiles: a raster (or the arena of the reference worker),
+// the chip of pair p at ref_base + ref_off[p] with row stride ref_stride pixels, the search
+// window at tgt_base + tgt_off[p] with row stride tgt_stride
+struct PairSource {
+    const float2* ref_base;
+    const long long* ref_off;
+    long long ref_stride;
+    const float2* tgt_base;
+    const long long* tgt_off;
+    long long tgt_stride;
+};
+
+// coarse result of one pair
+struct CoarseOut {
+    int u, v;          // argmax placement
+    int top, left;     // nudged corner of the refinement neighbourhood inside the window
+};
+
+// optional per-pair diagnostics (matches ampcor_pair_diag in the public header)
+struct PairDiag {
+    int coarse_u, coarse_v;
+    int top, left;
+    int refined_u, refined_v;
+    int fine_p, fine_q;
+    float coarse_peak;
+    float refined_peak;
+    float zoom_peak;
+    float pad;
+};
+
+__global__ void pair_offsets_kernel(const int* ulhc, long long pairs, long long ref_lines,
+                                    long long ref_samples, long long tgt_lines,
+                                    long long tgt_samples, int R, int W, long long* ref_off,
+                                    long long* tgt_off, unsigned int* bad);
+
+__global__ void arena_offsets_kernel(long long pairs, long long ref_cells, long long tgt_cells,
+                                     long long* ref_off, long long* tgt_off);
+
+__global__ void coarse_kernel(PairSource src, long long pair0, long long pairs, NccGeom g, int m,
+                              CoarseOut* out, float* coarse_peak, float* surfaces);
+
+__global__ void refine_kernel(PairSource src, long long pair0, long long pairs,
+                              const CoarseOut* coarse, InterpGeom chip_g, InterpGeom win_g,
+                              const float* chip_taps, const float* win_taps, float* refined,
+                              long long refined_stride);
+
+__global__ void fine_kernel(const float* refined, long long refined_stride, long long pair0,
+                            long long pairs, const long long* ref_off, NccGeom g, ZoomGeom zg,
+                            const float* zoom_taps, const CoarseOut* coarse,
+                            const float* coarse_peak, int margin, int refine_factor,
+                            int refine_margin, int ref_compat, float2* offsets, PairDiag* diag,
+                            float* surfaces);
+
+}  // namespace ampcor_b200

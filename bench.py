@@ -1,0 +1,370 @@
+"""Benchmark of the batched tile correlator (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
+
+A step is one full correlation job: every tile pair of the workload (default
+production_4096: 4096x4096 complex64 speckle pair, 14,400 pairs of 64x64 chips, +-32 px search,
+refine factor 2 with an 8 px refine margin, zoom 8) run through the CUDA pipeline with rasters,
+pair corners and outputs resident in HBM.  Under torchrun every rank correlates its own job of
+the same size on its own GPU (weak scaling, no collective on the data path); ``value`` is the
+pairs of all ranks divided by the slowest rank's device time.
+
+``e2e`` is the same metric through the host entry point of the C ABI
+(ampcor_correlate_host): each step uploads both rasters and the corners from pinned host
+memory, runs the job and reads the offsets back.
+
+``--impl reference`` times the CPU implementation of the path instead: the FP64 restatement of
+the reference pipeline in oracle/ (the reference itself cannot be built here: it needs the pyre
+framework), with all host threads, on a bounded sample of the same pairs each step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "tile pairs/s (64² chip, ±32 px search) & p99 job latency at ≤0.01 px error"
+UNIT = "tile pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="production_4096")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def workload_config(w):
+    return {
+        "workload": (f"{w.name}: {w.ref.shape[0]}x{w.ref.shape[1]} complex64 raster pair, "
+                     f"{w.pairs} pairs of {w.chip}x{w.chip} chips, +-{w.margin} px search, "
+                     f"refine {w.refine_factor} (margin {w.refine_margin}), zoom {w.zoom_factor}"),
+        "pairs_per_gpu": w.pairs,
+        "chip": w.chip,
+        "search_margin": w.margin,
+        "refine_factor": w.refine_factor,
+        "refine_margin": w.refine_margin,
+        "zoom_factor": w.zoom_factor,
+        "l2": "inputs larger than L2 (two 134 MB rasters per job; L2 is 126 MB)",
+    }
+
+
+def oracle_rate(w, seconds, threads):
+    """Pairs/s of the FP64 CPU pipeline on a bounded sample of the workload's pairs."""
+    import oracle
+
+    rng = np.random.default_rng(0)
+    order = rng.permutation(w.pairs)
+    probe = order[: max(threads, 8)]
+    t0 = time.perf_counter()
+    oracle.adjust(w.ref, w.tgt, w.ulhc[probe], w.chip, w.window, w.refine_factor,
+                  w.refine_margin, w.zoom_factor, threads=threads)
+    per = (time.perf_counter() - t0) / len(probe)
+    n = int(min(w.pairs, max(len(probe), seconds / max(per, 1e-9))))
+    n = max(threads, (n // threads) * threads) if n >= threads else n
+    sample = np.sort(order[:n])
+    t0 = time.perf_counter()
+    oracle.adjust(w.ref, w.tgt, w.ulhc[sample], w.chip, w.window, w.refine_factor,
+                  w.refine_margin, w.zoom_factor, threads=threads)
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.6)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp32_peak(device):
+    import ctypes
+
+    path = os.path.join(ROOT, "ampcor_b200", "libampcor_peak.so")
+    lib = ctypes.CDLL(path)
+    lib.fp32_fma_tflops.restype = ctypes.c_double
+    lib.fp32_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+    return lib.fp32_fma_tflops(device, 5)
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return {}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from ampcor_b200 import synth
+
+    w = synth.workload(args.workload)
+    threads = os.cpu_count() or 1
+    total_budget = 150.0
+    per_step = max(2.0, total_budget / max(1, args.steps + args.warmup))
+    rates, samples = [], []
+    for i in range(args.warmup + args.steps):
+        r, n, dt = oracle_rate(w, per_step, threads)
+        if i >= args.warmup:
+            rates.append(r)
+            samples.append(n)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * w.pairs / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(w),
+        "cpu_baseline": {
+            "value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"FP64 restatement of the full reference pipeline (oracle/oracle.c: coarse "
+                       f"NCC, nudge, FFT refinement, refined NCC, zoom, offsets), OpenMP over pairs "
+                       f"on {threads} threads, {samples[0]} random pairs of the workload per step "
+                       f"(median of {len(rates)} steps)"),
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from ampcor_b200 import synth
+    from ampcor_b200.worker import Worker
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    w = synth.workload(args.workload)
+    worker = Worker(pairs=w.pairs, chip=(w.chip, w.chip), window=(w.window, w.window),
+                    refine_factor=w.refine_factor, refine_margin=w.refine_margin,
+                    zoom_factor=w.zoom_factor, device=local)
+    ref = torch.from_numpy(w.ref).to(dev)
+    tgt = torch.from_numpy(w.tgt).to(dev)
+    ulhc = torch.from_numpy(w.ulhc).to(dev)
+    offsets = torch.empty((w.pairs, 2), dtype=torch.float32, device=dev)
+
+    def step():
+        worker.correlate(ref, tgt, ulhc, offsets=offsets, synchronize=False)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    worker.profile(True)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    coarse_ms, refine_ms, fine_ms, launches = worker.stage_times()
+    worker.profile(False)
+    clk = clocks.stop()
+    # result check outside the timed region
+    worker._lib.ampcor_synchronize(worker.handle, None)
+    ok = bool(torch.isfinite(offsets).all().item())
+
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * w.pairs * args.steps / (ms_max / 1000.0)
+
+    # end to end through the host entry point, pinned host buffers
+    ref_h = torch.empty(w.ref.shape, dtype=torch.complex64, pin_memory=True)
+    tgt_h = torch.empty(w.tgt.shape, dtype=torch.complex64, pin_memory=True)
+    ulhc_h = torch.empty(w.ulhc.shape, dtype=torch.int32, pin_memory=True)
+    ref_h.numpy()[...] = w.ref
+    tgt_h.numpy()[...] = w.tgt
+    ulhc_h.numpy()[...] = w.ulhc
+    rn, tn, un = ref_h.numpy(), tgt_h.numpy(), ulhc_h.numpy()
+    worker.correlate(rn, tn, un)
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        out = worker.correlate(rn, tn, un)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * w.pairs * e2e_steps / float(te.item())
+    ok = ok and bool(np.isfinite(out).all())
+
+    line = None
+    if rank == 0:
+        per_launch_pairs_fine = min(worker_chunk(), w.pairs)
+        n_chunks = -(-w.pairs // per_launch_pairs_fine)
+        C = w.window - w.chip + 1
+        Rf = w.refine_factor * w.chip
+        Cf = 2 * w.refine_factor * w.refine_margin + 1
+        flop_coarse = 2.0 * w.chip ** 2 * C ** 2
+        flop_fine = 2.0 * Rf ** 2 * Cf ** 2
+        stage = {"coarse_kernel": coarse_ms, "refine_kernel": refine_ms, "fine_kernel": fine_ms}
+        top = max(stage, key=stage.get)
+        if top == "coarse_kernel":
+            per_launch_ms = coarse_ms / args.steps
+            flops = flop_coarse * w.pairs
+        elif top == "fine_kernel":
+            per_launch_ms = fine_ms / (args.steps * n_chunks)
+            flops = flop_fine * per_launch_pairs_fine
+        else:
+            per_launch_ms = refine_ms / (args.steps * n_chunks)
+            flops = flop_fine * per_launch_pairs_fine  # not a contraction; reported for scale
+        achieved = flops / (per_launch_ms / 1000.0) / 1e12
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        tensor_peak = peaks.get("bf16_tflops")
+        peak_src = "of measured" if tensor_peak else "of fallback"
+        tensor_peak = tensor_peak or 1590.0
+        simt = fp32_peak(local)
+        traffic = load_traffic().get(top)
+        traffic_per_launch = None
+        if traffic:
+            units = w.pairs if top == "coarse_kernel" else per_launch_pairs_fine
+            traffic_per_launch = traffic["bytes_per_pair"] * units
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            rate, n, dt = oracle_rate(w, args.cpu_seconds, threads)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": (f"FP64 restatement of the full reference pipeline (oracle/oracle.c) "
+                              f"on {n} random pairs of the workload, {dt:.1f} s on {threads} "
+                              f"threads")}
+        h2d = w.ref.nbytes + w.tgt.nbytes + w.ulhc.nbytes
+        d2h = w.pairs * 2 * 4
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(w),
+            "roofline": {
+                "bound": "tensor", "kernel": top, "achieved": achieved, "peak": tensor_peak,
+                "unit": "TFLOP/s", "frac": achieved / tensor_peak, "traffic": traffic_per_launch,
+                "peak_note": (f"dense bf16 tensor peak {peak_src} (MEASURED_PEAKS.json burst); "
+                              f"the plain form runs on the FP32 pipes"),
+                "fp32_simt_peak": simt, "fp32_simt_frac": achieved / simt if simt > 0 else None,
+                "algorithmic_flop_per_launch": flops, "ms_per_launch": per_launch_ms,
+                "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": int(launches + args.steps),  # + the corner-offset kernel per step
+            "clocks": clk,
+            "results_finite": ok,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    worker.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def worker_chunk():
+    env = os.environ.get("AMPCOR_CHUNK")
+    return int(env) if env and int(env) > 0 else 148 * 4
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * ampcor_b200: C ABI of the B200 (sm_100a) batched tile correlator.
+ *
+ * This is the drop-in boundary for the CUDA worker of ampcor.  Each entry point names the
+ * reference interface it replaces (paths inside the isce-framework/ampcor source tree).
+ * Every function returns AMPCOR_OK (0) or one of the AMPCOR_E_* codes and never throws; the
+ * message of the last failure on a handle is available from ampcor_last_error().
+ * All pointers are plain pointers; nothing here needs a C++ or PyTorch type.
+ */
+#ifndef AMPCOR_B200_H
+#define AMPCOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the reference raises std::bad_alloc / std::runtime_error / std::logic_error
+   from its launchers, e.g. lib/libampcor_cuda/correlators/Sequential.icc:301-335) */
+#define AMPCOR_OK 0
+#define AMPCOR_E_ARG 1      /* invalid argument (null pointer, pair id out of range, ...) */
+#define AMPCOR_E_SHAPE 2    /* tile geometry this build does not support */
+#define AMPCOR_E_CUDA 3     /* CUDA runtime failure */
+#define AMPCOR_E_NOMEM 4    /* host or device allocation failure */
+#define AMPCOR_E_BOUNDS 5   /* a chip or window leaves its raster (the pair's offsets are NaN) */
+#define AMPCOR_E_STATE 6    /* call out of order */
+
+/* ampcor_params.flags */
+#define AMPCOR_FLAG_REF_COMPAT 1u  /* assemble offsets with the reference formula, which
+                                      subtracts the refine margin a second time
+                                      (lib/libampcor_cuda/correlators/offsets.cu:124-125) */
+
+typedef struct ampcor_handle ampcor_handle;
+
+/*
+ * Worker geometry.  Replaces the arguments of the reference worker constructor
+ * Sequential(pairs, refLayout, tgtLayout, refineFactor, refineMargin, zoomFactor)
+ * (lib/libampcor_cuda/correlators/Sequential.h:64-67) as parsed by the extension's
+ * sequential(points, (refLines, refSamples), (tgtLines, tgtSamples), refineMargin,
+ * refineFactor, zoomFactor) (ext/ampcor_cuda/sequential.cc:40-73).
+ * Tiles are square (ref_lines == ref_samples, tgt_lines == tgt_samples), as the reference
+ * assumes (Sequential.icc:55-60); the search margin is (tgt - ref) / 2.
+ */
+typedef struct {
+    uint64_t pairs;          /* number of tile pairs of the arena API (capacity) */
+    uint64_t ref_lines;      /* chip shape */
+    uint64_t ref_samples;
+    uint64_t tgt_lines;      /* search window shape */
+    uint64_t tgt_samples;
+    uint64_t refine_factor;  /* upsampling factor of the refinement (reference default 2) */
+    uint64_t refine_margin;  /* refinement margin around the coarse peak (default 8) */
+    uint64_t zoom_factor;    /* zoom factor of the refined correlation surface */
+    int32_t device;          /* CUDA device ordinal */
+    uint32_t flags;          /* AMPCOR_FLAG_* */
+} ampcor_params;
+
+/* per-pair diagnostics of the last run */
+typedef struct {
+    int32_t coarse_u, coarse_v;    /* coarse correlation maximum (placement row, column) */
+    int32_t top, left;             /* nudged corner of the refinement neighbourhood */
+    int32_t refined_u, refined_v;  /* refined correlation maximum */
+    int32_t fine_p, fine_q;        /* maximum of the zoomed surface */
+    float coarse_peak;             /* coarse correlation maximum value */
+    float refined_peak;            /* refined correlation maximum value (peak correlation) */
+    float zoom_peak;               /* zoomed surface maximum value */
+    float reserved;
+} ampcor_pair_diag;
+
+/*
+ * A batch of tile pairs cut from two complex64 rasters (row-major, lines x samples, the SLC
+ * layout of lib/libampcor/dom/SLC.icc:123-126).  Replaces the host tile arena filled pair by
+ * pair (pkg/ampcor/correlators/CUDA.py:50-54) with a gather on the device: pair p correlates the
+ * chip whose upper-left pixel is (ulhc[4p], ulhc[4p+1]) in ref against the search window whose
+ * upper-left pixel is (ulhc[4p+2], ulhc[4p+3]) in tgt (Plan.py:160-170 computes these corners).
+ */
+typedef struct {
+    const void* ref;            /* complex64 reference raster */
+    int64_t ref_lines, ref_samples;
+    const void* tgt;            /* complex64 secondary raster */
+    int64_t tgt_lines, tgt_samples;
+    const int32_t* ulhc;        /* 4 int32 per pair */
+    uint64_t pairs;
+    float* offsets;             /* out: 2 floats per pair, (dy, dx) */
+    ampcor_pair_diag* diag;     /* out, optional */
+    float* coarse_surfaces;     /* out, optional: pairs x C^2 coarse correlation surfaces */
+    float* refined_surfaces;    /* out, optional: pairs x Cf^2 refined correlation surfaces */
+} ampcor_job;
+
+/* Create a worker bound to params->device.  Replaces Sequential<raster_t>::Sequential
+   (lib/libampcor_cuda/correlators/Sequential.icc:173-234) and the extension's
+   sequential() (ext/ampcor_cuda/sequential.cc:40-73). */
+int ampcor_create(const ampcor_params* params, ampcor_handle** handle);
+
+/* Release the worker and all its memory.  Replaces the capsule destructor
+   (ext/ampcor_cuda/sequential.cc:274-286) and Sequential::~Sequential (Sequential.icc:160-170). */
+int ampcor_destroy(ampcor_handle* handle);
+
+/* Copy the R x R complex64 chip of pair pid (row stride in pixels) into the worker's arena.
+   Replaces Sequential::addReferenceTile (Sequential.icc:15-28) and the extension's
+   addReference() (ext/ampcor_cuda/sequential.cc:85-143). */
+int ampcor_add_reference(ampcor_handle* handle, uint64_t pid, const void* tile,
+                         uint64_t row_stride);
+
+/* Copy the W x W complex64 search window of pair pid.  Replaces Sequential::addTargetTile
+   (Sequential.icc:31-44) and addTarget() (ext/ampcor_cuda/sequential.cc:155-213). */
+int ampcor_add_target(ampcor_handle* handle, uint64_t pid, const void* tile,
+                      uint64_t row_stride);
+
+/* Correlate every pair of the arena and return the offset field: 2 floats per pair, (dy, dx) in
+   pair order, owned by the worker and valid until the next adjust or destroy.  Replaces
+   Sequential::adjust (Sequential.icc:47-141) and the extension's adjust()
+   (ext/ampcor_cuda/sequential.cc:225-271). */
+int ampcor_adjust(ampcor_handle* handle, const float** offsets);
+
+/* Copy the per-pair diagnostics of the last ampcor_adjust into host memory (pairs entries).
+   No reference counterpart (the reference keeps no per-pair record). */
+int ampcor_diagnostics(ampcor_handle* handle, ampcor_pair_diag* diag);
+
+/* Correlate a batch given device-resident rasters, corners and outputs; enqueued on stream
+   (a cudaStream_t, NULL for the worker's own stream) without waiting.  Replaces the arena
+   push and adjust (Sequential.icc:291-339, :47-141) with a device-side tile gather.  Pairs
+   whose tiles leave a raster get NaN offsets and make the next ampcor_synchronize() return
+   AMPCOR_E_BOUNDS. */
+int ampcor_correlate(ampcor_handle* handle, const ampcor_job* job, void* stream);
+
+/* Wait for the work enqueued on the worker's stream (or stream, when not NULL) and report
+   any bounds failure of the batches since the last call. */
+int ampcor_synchronize(ampcor_handle* handle, void* stream);
+
+/* Same as ampcor_correlate but every pointer of job is host memory: the call uploads the
+   rasters and corners, runs the batch and copies the offsets (and optional outputs) back before
+   it returns.  This is the end-to-end path of pkg/ampcor/correlators/CUDA.py:22-61. */
+int ampcor_correlate_host(ampcor_handle* handle, const ampcor_job* job);
+
+/* Placements per axis of the coarse (C = W - R + 1) and refined (Cf = 2 f m + 1) surfaces and
+   the zoomed surface dimension (Z = z Cf), for sizing the optional outputs. */
+int ampcor_surface_dims(const ampcor_handle* handle, int32_t* coarse, int32_t* refined,
+                        int32_t* zoomed);
+
+/* Switch per-stage timing on (enable != 0) or off.  While on, every batch records CUDA events
+   around each kernel launch on the batch's stream.  No reference counterpart (the reference
+   prints wall-clock stage times to a debug journal channel, e.g. tests/libampcor_cuda/
+   correlate.cc). */
+int ampcor_profile(ampcor_handle* handle, int enable);
+
+/* Device time (milliseconds) spent in the coarse, refinement and fine kernels and the number of
+   those kernel launches since profiling was switched on or last read; waits for the recorded
+   events and resets the counters. */
+int ampcor_stage_times(ampcor_handle* handle, double* coarse_ms, double* refine_ms,
+                       double* fine_ms, uint64_t* launches);
+
+/* Message of the last failure on handle (or of the last failed ampcor_create when handle is
+   NULL). */
+const char* ampcor_last_error(const ampcor_handle* handle);
+
+/* Replace the extension's version() and copyright() (ext/ampcor_cuda/ampcor_cuda.cc:25-27). */
+const char* ampcor_version(void);
+const char* ampcor_copyright(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMPCOR_B200_H */

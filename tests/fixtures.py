@@ -1,0 +1,27 @@
+"""Restated fixtures of the reference's stage tests.
+
+placement_identity(R, M, seed): the fixture of tests/libampcor_cuda/correlate.cc:119-143 (and
+maxcor.cc, tgtStats.cc, nudge.cc): one random-normal real chip; (2M+1)^2 pairs, pair (i, j)
+has an all-zero (R+2M)^2 window with the chip pasted at (i, j).  The reference seeds from
+std::random_device; here the seed is fixed.  Returned as rasters + corners so the same data
+feeds the oracle and the CUDA path: the chip raster is R x R; the window raster stacks the
+(2M+1)^2 windows vertically.
+"""
+import numpy as np
+
+
+def placement_identity(R, M, seed=0):
+    W = R + 2 * M
+    C = 2 * M + 1
+    rng = np.random.default_rng(seed)
+    chip = rng.standard_normal((R, R)).astype(np.float32)
+    ref = chip.astype(np.complex64)
+    pairs = C * C
+    tgt = np.zeros((pairs * W, W), np.complex64)
+    ulhc = np.zeros((pairs, 4), np.int32)
+    for i in range(C):
+        for j in range(C):
+            pid = i * C + j
+            tgt[pid * W + i: pid * W + i + R, j: j + R] = chip
+            ulhc[pid] = (0, 0, pid * W, 0)
+    return ref, tgt, ulhc

@@ -1,0 +1,208 @@
+"""Parity of the CUDA path with the oracle (needs a B200).
+
+Tolerances:
+* integer (coarse) offsets: bit-exact against the reference CPU correlator
+  (oracle.coarse_cpu) for every pair whose top-two coarse correlation gap exceeds 1e-5
+  (FP32 surfaces are within ~1e-6 of FP64);
+* sub-pixel offsets: the same zoom-grid cell as the FP64 oracle (so the offsets are equal), for
+  every pair whose zoomed-surface top-two gap exceeds 1e-5;
+* peak correlation (refined surface maximum): within 1e-5 relative of the oracle;
+* correlation surfaces: within 2e-5 absolute of the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from ampcor_b200 import synth
+from ampcor_b200.worker import DIAG_DTYPE, Error, Worker
+from ampcor_b200.ext import ampcor_cuda
+
+from fixtures import placement_identity
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GAP = 1e-5
+PEAK_RTOL = 1e-5
+SURF_ATOL = 2e-5
+
+
+def run_device(w: synth.Workload, ulhc=None, surfaces=False):
+    ulhc = w.ulhc if ulhc is None else ulhc
+    worker = Worker(pairs=len(ulhc), chip=(w.chip, w.chip), window=(w.window, w.window),
+                    refine_factor=w.refine_factor, refine_margin=w.refine_margin,
+                    zoom_factor=w.zoom_factor)
+    dev = torch.device("cuda:0")
+    ref = torch.from_numpy(w.ref).to(dev)
+    tgt = torch.from_numpy(w.tgt).to(dev)
+    u = torch.from_numpy(np.ascontiguousarray(ulhc)).to(dev)
+    P = len(ulhc)
+    diag = torch.zeros((P, DIAG_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    cs = rs = None
+    if surfaces:
+        cs = torch.zeros((P, worker.coarse_dim, worker.coarse_dim), dtype=torch.float32, device=dev)
+        rs = torch.zeros((P, worker.refined_dim, worker.refined_dim), dtype=torch.float32, device=dev)
+    off = worker.correlate(ref, tgt, u, diag=diag, coarse_surfaces=cs, refined_surfaces=rs)
+    out = dict(offsets=off.cpu().numpy(), diag=diag.cpu().numpy().view(DIAG_DTYPE).reshape(P))
+    if surfaces:
+        out["coarse"] = cs.cpu().numpy()
+        out["refined"] = rs.cpu().numpy()
+    worker.close()
+    return out
+
+
+def check_parity(w, ulhc, gpu, label):
+    R, W = w.chip, w.window
+    off, od = oracle.adjust(w.ref, w.tgt, ulhc, R, W, w.refine_factor, w.refine_margin,
+                            w.zoom_factor)
+    arg, gap = oracle.coarse_cpu(w.ref, w.tgt, ulhc, R, W)
+    d = gpu["diag"]
+    # integer offsets against the reference CPU correlator
+    safe = gap > GAP
+    assert safe.mean() > 0.95, f"{label}: too many near-tie coarse surfaces"
+    assert np.array_equal(d["coarse_u"][safe], arg[safe, 0]), label
+    assert np.array_equal(d["coarse_v"][safe], arg[safe, 1]), label
+    # coarse argmax of the intended pipeline (mean-removed chip) is the same cell
+    assert np.array_equal(od["coarse_u"], arg[:, 0]) and np.array_equal(od["coarse_v"], arg[:, 1])
+    # nudged corners follow
+    same_coarse = (d["coarse_u"] == od["coarse_u"]) & (d["coarse_v"] == od["coarse_v"])
+    assert np.array_equal(d["top"][same_coarse], od["top"][same_coarse])
+    assert np.array_equal(d["left"][same_coarse], od["left"][same_coarse])
+    # sub-pixel: same zoom-grid cell where the oracle's zoomed surface has a clear maximum
+    zsafe = same_coarse & (od["zoom_gap"] > GAP)
+    assert zsafe.mean() > 0.95, f"{label}: too many near-tie zoomed surfaces"
+    assert np.array_equal(d["fine_p"][zsafe], od["fine_p"][zsafe]), label
+    assert np.array_equal(d["fine_q"][zsafe], od["fine_q"][zsafe]), label
+    assert np.array_equal(gpu["offsets"][zsafe], off[zsafe]), label
+    # every offset, tie or not, is within one zoom quantum of the oracle
+    quantum = 1.0 / (w.refine_factor * w.zoom_factor)
+    assert np.abs(gpu["offsets"][same_coarse] - off[same_coarse]).max() <= quantum + 1e-6
+    # peak correlation
+    np.testing.assert_allclose(d["refined_peak"][same_coarse], od["refined_peak"][same_coarse],
+                               rtol=PEAK_RTOL, atol=0)
+    np.testing.assert_allclose(d["coarse_peak"], od["coarse_peak"], rtol=PEAK_RTOL, atol=0)
+    return off, od
+
+
+def test_plain_512_parity():
+    w = synth.plain_512()
+    gpu = run_device(w, surfaces=True)
+    off, od, cs, rs = oracle.adjust(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4, surfaces=True)
+    check_parity(w, w.ulhc, gpu, "plain_512")
+    assert np.all(gpu["offsets"] == np.float32([3.375, -2.75]))
+    np.testing.assert_allclose(gpu["coarse"], cs, atol=SURF_ATOL, rtol=0)
+    np.testing.assert_allclose(gpu["refined"], rs, atol=SURF_ATOL, rtol=0)
+
+
+def test_golden_plain_512_on_gpu():
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "plain_512.npz"))
+    gpu = run_device(synth.plain_512())
+    assert np.array_equal(gpu["offsets"], g["offsets"])
+    assert np.array_equal(gpu["diag"]["coarse_u"], g["coarse_cpu_argmax"][:, 0])
+    assert np.array_equal(gpu["diag"]["coarse_v"], g["coarse_cpu_argmax"][:, 1])
+
+
+@pytest.mark.parametrize("R,M", [(32, 8), (64, 32)])
+def test_placement_identity(R, M):
+    # correlate.cc:279-303 (gamma = 1 at the placement, 10 eps_f in FP32 there; FP32 sums of
+    # R^2 terms here, so 1e-5), maxcor.cc:296-312 (argmax = placement), nudge.cc:204-225
+    ref, tgt, ulhc = placement_identity(R, M, seed=5)
+    W, C = R + 2 * M, 2 * M + 1
+    w = synth.Workload("identity", ref, tgt, ulhc, np.zeros((len(ulhc), 2)), R, M, 2,
+                       min(4, M), 4, None)
+    gpu = run_device(w, surfaces=True)
+    d = gpu["diag"]
+    i, j = np.divmod(np.arange(C * C), C)
+    assert np.array_equal(d["coarse_u"], i) and np.array_equal(d["coarse_v"], j)
+    np.testing.assert_allclose(gpu["coarse"][np.arange(C * C), i, j], 1.0, atol=1e-5)
+    E = R + 2 * w.refine_margin
+    assert d["top"].min() >= 0 and d["top"].max() <= W - E
+    assert d["left"].min() >= 0 and d["left"].max() <= W - E
+
+
+def _subset(w, n, seed=0):
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(w.pairs, size=n, replace=False))
+    return idx
+
+
+def test_production_subset_parity():
+    w = synth.production_4096()
+    idx = _subset(w, 192)
+    gpu = run_device(w, ulhc=w.ulhc[idx])
+    check_parity(w, w.ulhc[idx], gpu, "production_4096")
+
+
+def test_heavy_tail_subset_parity():
+    w = synth.production_4096(heavy_tail=True)
+    idx = _subset(w, 128, seed=1)
+    gpu = run_device(w, ulhc=w.ulhc[idx])
+    check_parity(w, w.ulhc[idx], gpu, "heavy_tail_4096")
+
+
+def test_production_full_size_properties():
+    # all 14,400 pairs: finite, near the applied field, and each result identical whether the
+    # pair runs in the full batch or in a small one (no cross-pair dependence)
+    w = synth.production_4096()
+    full = run_device(w)
+    assert np.isfinite(full["offsets"]).all()
+    err = np.abs(full["offsets"] - w.truth)
+    assert np.quantile(err, 0.99) < 0.2
+    idx = _subset(w, 300, seed=2)
+    part = run_device(w, ulhc=w.ulhc[idx])
+    assert np.array_equal(part["offsets"], full["offsets"][idx])
+    assert np.array_equal(part["diag"], full["diag"][idx])
+    again = run_device(w)
+    assert np.array_equal(again["offsets"], full["offsets"])
+
+
+def test_host_path_matches_device_path():
+    w = synth.plain_512()
+    worker = Worker(pairs=w.pairs, chip=(32, 32), window=(48, 48), refine_factor=2,
+                    refine_margin=4, zoom_factor=4)
+    off, diag = worker.correlate(w.ref, w.tgt, w.ulhc, diag=True)
+    dev = run_device(w)
+    assert np.array_equal(off, dev["offsets"])
+    assert np.array_equal(diag, dev["diag"])
+
+
+def test_extension_mirror_matches_raster_path():
+    # the reference's call sequence (pkg/ampcor/correlators/CUDA.py:45-58)
+    w = synth.plain_512()
+    worker = ampcor_cuda.sequential(w.pairs, (32, 32), (48, 48), 4, 2, 4)
+    for idx, (rl, rs, tl, ts) in enumerate(w.ulhc):
+        ampcor_cuda.addReference(worker, w.ref, idx, (rl, rs), (rl + 32, rs + 32))
+        ampcor_cuda.addTarget(worker, w.tgt, idx, (tl, ts), (tl + 48, ts + 48))
+    offsets = ampcor_cuda.adjust(worker)
+    assert isinstance(offsets, tuple) and len(offsets) == w.pairs
+    assert all(isinstance(o, tuple) and len(o) == 2 for o in offsets)
+    dev = run_device(w)
+    assert np.array_equal(np.array(offsets, np.float32), dev["offsets"])
+
+
+def test_ref_compat_flag():
+    w = synth.plain_512()
+    worker = Worker(pairs=w.pairs, chip=(32, 32), window=(48, 48), refine_factor=2,
+                    refine_margin=4, zoom_factor=4, ref_compat=True)
+    off = worker.correlate(w.ref, w.tgt, w.ulhc)
+    oc, _ = oracle.adjust(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4, ref_compat=True)
+    assert np.array_equal(off, oc)
+
+
+def test_out_of_bounds_pair_reports_and_is_nan():
+    w = synth.plain_512()
+    ulhc = w.ulhc[:4].copy()
+    ulhc[2, 2] = 500   # window leaves the 512-line raster
+    worker = Worker(pairs=4, chip=(32, 32), window=(48, 48), refine_factor=2, refine_margin=4,
+                    zoom_factor=4)
+    dev = torch.device("cuda:0")
+    with pytest.raises(Error) as e:
+        worker.correlate(torch.from_numpy(w.ref).to(dev), torch.from_numpy(w.tgt).to(dev),
+                         torch.from_numpy(ulhc).to(dev))
+    assert "leave their raster" in str(e.value)
+    off = worker.correlate(torch.from_numpy(w.ref).to(dev), torch.from_numpy(w.tgt).to(dev),
+                           torch.from_numpy(ulhc).to(dev), synchronize=False)
+    torch.cuda.synchronize()
+    o = off.cpu().numpy()
+    assert np.isnan(o[2]).all() and np.isfinite(o[[0, 1, 3]]).all()
