@@ -443,12 +443,15 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     };
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return cuda_create_fail(e, "creating the worker stream");
+    // the opt-in limit is per kernel and process-wide: raise it to the device maximum once so
+    // that workers of different geometries can coexist
+    const int kMaxSmem = 227 * 1024;
     if ((e = cudaFuncSetAttribute(coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  h->gc.smem_bytes)) != cudaSuccess ||
+                                  kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  h->gf.smem_bytes)) != cudaSuccess ||
+                                  kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  h->refine_smem)) != cudaSuccess)
+                                  kMaxSmem)) != cudaSuccess)
         return cuda_create_fail(e, "configuring kernel shared memory");
 
     const std::vector<float> ct = taps_table(h->R, h->f, 1, h->ic.taps_len);
