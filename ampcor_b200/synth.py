@@ -22,7 +22,8 @@ import numpy as np
 from .plan import constant_codomain, plan_pairs, uniform_grid
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CACHE = os.path.join(os.path.dirname(HERE), ".synth_cache")
+# generated rasters are cached per machine, outside the source tree
+CACHE = os.environ.get("AMPCOR_SYNTH_CACHE", os.path.join("/tmp", "ampcor_b200_synth"))
 
 
 def speckle(shape, seed) -> np.ndarray:

@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--workload", default="production_4096")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--pairs", type=int, default=0,
+                    help="correlate only the first N pairs (small cases for profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -213,6 +216,9 @@ def run_b200(args):
                                 device_id=dev)
 
     w = synth.workload(args.workload)
+    if args.pairs:
+        w.ulhc = w.ulhc[: args.pairs]
+        w.truth = None if w.truth is None else w.truth[: args.pairs]
     worker = Worker(pairs=w.pairs, chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
                     zoom_factor=w.zoom_factor, device=local)
@@ -259,25 +265,27 @@ def run_b200(args):
     value = world * w.pairs * args.steps / (ms_max / 1000.0)
 
     # end to end through the host entry point, pinned host buffers
-    ref_h = torch.empty(w.ref.shape, dtype=torch.complex64, pin_memory=True)
-    tgt_h = torch.empty(w.tgt.shape, dtype=torch.complex64, pin_memory=True)
-    ulhc_h = torch.empty(w.ulhc.shape, dtype=torch.int32, pin_memory=True)
-    ref_h.numpy()[...] = w.ref
-    tgt_h.numpy()[...] = w.tgt
-    ulhc_h.numpy()[...] = w.ulhc
-    rn, tn, un = ref_h.numpy(), tgt_h.numpy(), ulhc_h.numpy()
-    worker.correlate(rn, tn, un)
-    e2e_steps = max(3, min(args.steps, 10))
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        out = worker.correlate(rn, tn, un)
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * w.pairs * e2e_steps / float(te.item())
-    ok = ok and bool(np.isfinite(out).all())
+    e2e_value, e2e_steps = None, 0
+    if not args.no_e2e:
+        ref_h = torch.empty(w.ref.shape, dtype=torch.complex64, pin_memory=True)
+        tgt_h = torch.empty(w.tgt.shape, dtype=torch.complex64, pin_memory=True)
+        ulhc_h = torch.empty(w.ulhc.shape, dtype=torch.int32, pin_memory=True)
+        ref_h.numpy()[...] = w.ref
+        tgt_h.numpy()[...] = w.tgt
+        ulhc_h.numpy()[...] = w.ulhc
+        rn, tn, un = ref_h.numpy(), tgt_h.numpy(), ulhc_h.numpy()
+        worker.correlate(rn, tn, un)
+        e2e_steps = max(3, min(args.steps, 10))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            out = worker.correlate(rn, tn, un)
+        e2e_s = time.perf_counter() - t0
+        te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value = world * w.pairs * e2e_steps / float(te.item())
+        ok = ok and bool(np.isfinite(out).all())
 
     line = None
     if rank == 0:
@@ -338,8 +346,8 @@ def run_b200(args):
                 "algorithmic_flop_per_launch": flops, "ms_per_launch": per_launch_ms,
                 "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
             },
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                     "d2h_bytes_per_step": d2h, "steps": e2e_steps} if e2e_value else None),
             "gpu_launches": int(launches + args.steps),  # + the corner-offset kernel per step
             "clocks": clk,
             "results_finite": ok,
