@@ -99,6 +99,8 @@ SIGNATURES = {
     "ampcor_profile": (c_int, [c_void_p, c_int]),
     "ampcor_stage_times": (c_int, [c_void_p, POINTER(ctypes.c_double), POINTER(ctypes.c_double),
                                    POINTER(ctypes.c_double), POINTER(c_uint64)]),
+    "ampcor_correlate_noalloc": (c_int, [POINTER(Params), POINTER(Job), c_void_p, ctypes.c_char_p,
+                                         ctypes.c_size_t]),
     "ampcor_last_error": (c_char_p, [c_void_p]),
     "ampcor_version": (c_char_p, []),
     "ampcor_copyright": (c_char_p, []),

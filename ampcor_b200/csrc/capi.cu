@@ -728,3 +728,186 @@ const char* ampcor_version(void) { return kVersion; }
 const char* ampcor_copyright(void) { return kCopyright; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory while they run: applications that reserve the whole
+// GPU up front for their own memory pool (a caching allocator that owns every byte, so a stray
+// cudaMalloc fails or fragments it), and real-time or on-board processing chains that forbid any
+// allocation after start-up.  ampcor_correlate_noalloc() serves them: every intermediate of the
+// pipeline lives in the fixed device array below, which the CUDA runtime creates when it loads
+// this library on a device and keeps until the process exits (kNoAllocBytes on every device that
+// loads the library).  The array is shared by all calls; calls that overlap on the GPU race.
+// ------------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr long long kNoAllocMaxPairs = 16384;                // pairs per call
+constexpr long long kNoAllocTapFloats = 16384;               // interpolation tap tables
+constexpr long long kNoAllocRefinedBytes = 40ll << 20;       // refined amplitudes of a chunk
+constexpr long long kNoAllocTapsOff = 0;
+constexpr long long kNoAllocRefOff = kNoAllocTapsOff + kNoAllocTapFloats * 4;
+constexpr long long kNoAllocTgtOff = kNoAllocRefOff + kNoAllocMaxPairs * 8;
+constexpr long long kNoAllocCoarseOff = kNoAllocTgtOff + kNoAllocMaxPairs * 8;
+constexpr long long kNoAllocPeakOff = kNoAllocCoarseOff + kNoAllocMaxPairs * 16;
+constexpr long long kNoAllocBadOff = kNoAllocPeakOff + kNoAllocMaxPairs * 4;
+constexpr long long kNoAllocRefinedOff = kNoAllocBadOff + 256;
+constexpr long long kNoAllocBytes = kNoAllocRefinedOff + kNoAllocRefinedBytes;
+constexpr int kNoAllocMaxDevices = 64;
+
+static_assert(kNoAllocRefinedOff % 256 == 0, "scratch regions stay 256-byte aligned");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_base[kNoAllocMaxDevices] = {};
+float g_noalloc_taps[kNoAllocTapFloats];
+
+int noalloc_fail(char* errbuf, size_t errlen, int code, const char* what, cudaError_t e = cudaSuccess)
+{
+    if (errbuf && errlen) {
+        if (e != cudaSuccess)
+            std::snprintf(errbuf, errlen, "%s: %s", what, cudaGetErrorName(e));
+        else
+            std::snprintf(errbuf, errlen, "%s", what);
+    }
+    return code;
+}
+
+void taps_fill(int N, int f, int s0, int len, float* out)
+{
+    for (int s = s0; s < f; ++s)
+        for (int d = 0; d < len; ++d)
+            out[(size_t)(s - s0) * len + d] = (float)dirichlet(N, d - (N - 1) + (double)s / f);
+}
+
+}  // namespace
+
+extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job* j, void* stream,
+                                        char* errbuf, size_t errlen)
+{
+    if (errbuf && errlen) errbuf[0] = '\0';
+    if (!p || !j) return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "null argument");
+    if (p->ref_lines != p->ref_samples || p->tgt_lines != p->tgt_samples)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "chips and search windows must be square");
+    if (p->tgt_lines < p->ref_lines || (p->tgt_lines - p->ref_lines) % 2)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "window must exceed the chip by an even margin");
+    if (p->refine_factor < 1 || p->zoom_factor < 1 || p->ref_lines > 4096 || p->refine_factor > 16 ||
+        p->zoom_factor > 64 || p->refine_margin > 1024)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "geometry out of range");
+    if (j->pairs > (uint64_t)kNoAllocMaxPairs)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG,
+                            "ampcor_correlate_noalloc takes at most 16384 pairs per call");
+    if (j->pairs && (!j->ref || !j->tgt || !j->ulhc || !j->offsets))
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "null raster, corner or offset pointer");
+    if (j->ref_lines <= 0 || j->ref_samples <= 0 || j->tgt_lines <= 0 || j->tgt_samples <= 0)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "empty raster");
+    if (p->device < 0 || p->device >= kNoAllocMaxDevices)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "device ordinal out of range");
+
+    const int R = (int)p->ref_lines, W = (int)p->tgt_lines, f = (int)p->refine_factor;
+    const int m = (int)p->refine_margin, z = (int)p->zoom_factor;
+    const int E = R + 2 * m, Rf = f * R, Wf = f * E, Cf = 2 * f * m + 1, Z = z * Cf, M = (W - R) / 2;
+    if (E > W)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE,
+                            "refinement neighbourhood (chip + 2 * refine margin) exceeds the window");
+    ZoomGeom zg{};
+    zg.Cf = Cf;
+    zg.z = z;
+    zg.Z = Z;
+    zg.cb = 1;
+    for (int cb : {17, 13, 11, 5, 3})
+        if (Cf % cb == 0) {
+            zg.cb = cb;
+            break;
+        }
+    zg.taps_len = 2 * Cf + 32;
+    NccGeom gc{}, gf{};
+    InterpGeom ic{}, iw{};
+    std::string err;
+    if (!plan_ncc(R, W, 0, 0, gc, err) || !plan_ncc(Rf, Wf, Cf * Z, z * zg.taps_len, gf, err) ||
+        !plan_interp(R, f, ic, err) || !plan_interp(E, f, iw, err))
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "tile geometry not supported by this build");
+    const long long chip_taps = (long long)(f - 1) * ic.taps_len;
+    const long long win_taps = (long long)(f - 1) * iw.taps_len;
+    const long long zoom_taps = (long long)z * zg.taps_len;
+    if (chip_taps + win_taps + zoom_taps > kNoAllocTapFloats)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "interpolation tables exceed the fixed scratch");
+    const long long refined_stride = (long long)Rf * Rf + (long long)Wf * Wf;
+    const long long chunk = kNoAllocRefinedBytes / (refined_stride * 4);
+    if (chunk < 1)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_SHAPE, "refined tiles exceed the fixed scratch");
+
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "cudaSetDevice", e);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    // the device address of the fixed array, looked up once per device with that device current
+    if (!g_noalloc_base[p->device]) {
+        void* base = nullptr;
+        e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+        if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "cudaGetSymbolAddress", e);
+        g_noalloc_base[p->device] = base;
+    }
+    unsigned char* base = static_cast<unsigned char*>(g_noalloc_base[p->device]);
+    float* taps = reinterpret_cast<float*>(base + kNoAllocTapsOff);
+    long long* ref_off = reinterpret_cast<long long*>(base + kNoAllocRefOff);
+    long long* tgt_off = reinterpret_cast<long long*>(base + kNoAllocTgtOff);
+    CoarseOut* coarse = reinterpret_cast<CoarseOut*>(base + kNoAllocCoarseOff);
+    float* peak = reinterpret_cast<float*>(base + kNoAllocPeakOff);
+    unsigned int* bad = reinterpret_cast<unsigned int*>(base + kNoAllocBadOff);
+    float* refined = reinterpret_cast<float*>(base + kNoAllocRefinedOff);
+
+    const int kMaxSmem = 227 * 1024;
+    if ((e = cudaFuncSetAttribute(coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem)) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "configuring kernel shared memory", e);
+
+    // tap tables: computed on the host into a fixed buffer; a copy from pageable memory has left
+    // the buffer when cudaMemcpyAsync returns, so the buffer is free again under the lock
+    taps_fill(R, f, 1, ic.taps_len, g_noalloc_taps);
+    taps_fill(E, f, 1, iw.taps_len, g_noalloc_taps + chip_taps);
+    taps_fill(Cf, z, 0, zg.taps_len, g_noalloc_taps + chip_taps + win_taps);
+    if ((e = cudaMemcpyAsync(taps, g_noalloc_taps, (chip_taps + win_taps + zoom_taps) * sizeof(float),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "uploading interpolation taps", e);
+    // the bounds counter keeps the previous call's value: clear it
+    if ((e = cudaMemsetAsync(bad, 0, sizeof(unsigned int), st)) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "clearing the bounds counter", e);
+    if (j->pairs == 0) return AMPCOR_OK;
+
+    const long long P = (long long)j->pairs;
+    pair_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
+        j->ulhc, P, j->ref_lines, j->ref_samples, j->tgt_lines, j->tgt_samples, R, W, ref_off, tgt_off, bad);
+    PairSource src{static_cast<const float2*>(j->ref), ref_off, j->ref_samples,
+                   static_cast<const float2*>(j->tgt), tgt_off, j->tgt_samples};
+    coarse_kernel<<<(unsigned)P, kThreads, gc.smem_bytes, st>>>(src, 0, P, gc, m, coarse, peak,
+                                                                j->coarse_surfaces);
+    const int refine_smem = std::max(ic.smem_bytes, iw.smem_bytes);
+    for (long long c0 = 0; c0 < P; c0 += chunk) {
+        const long long n = std::min(chunk, P - c0);
+        refine_kernel<<<(unsigned)n, kThreads, refine_smem, st>>>(src, c0, n, coarse, ic, iw, taps,
+                                                                  taps + chip_taps, refined, refined_stride);
+        fine_kernel<<<(unsigned)n, kThreads, gf.smem_bytes, st>>>(
+            refined, refined_stride, c0, n, ref_off, gf, zg, taps + chip_taps + win_taps, coarse, peak, M, f,
+            m, (p->flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0, reinterpret_cast<float2*>(j->offsets),
+            reinterpret_cast<PairDiag*>(j->diag), j->refined_surfaces);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "launching the correlation kernels", e);
+    unsigned int nbad = 0;
+    if ((e = cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "running the correlation pipeline", e);
+    if (nbad)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_BOUNDS,
+                            "tile pair(s) leave their raster; their offsets are NaN");
+    return AMPCOR_OK;
+}

@@ -151,6 +151,22 @@ int ampcor_profile(ampcor_handle* handle, int enable);
 int ampcor_stage_times(ampcor_handle* handle, double* coarse_ms, double* refine_ms,
                        double* fine_ms, uint64_t* launches);
 
+/* Correlate a batch like ampcor_correlate(), but without allocating anything: for callers that
+   cannot allocate device memory while they run, such as applications whose own memory pool
+   already owns the whole GPU, or real-time and on-board processing chains that forbid
+   allocation after start-up.  No reference counterpart.
+   params gives the geometry and the device (params->pairs is ignored); every pointer of job is
+   device memory on that device; the work runs on stream (a cudaStream_t, NULL for the legacy
+   default stream) and the call waits for it.  All intermediates live in one fixed device array of
+   about 41 MiB that every device loading this library holds until the process exits; a call
+   takes at most 16384 pairs (more returns AMPCOR_E_ARG).  The first call on a device looks up the
+   array's device address, so make that first call before any stream capture.  All calls share
+   the array: calls that overlap on the GPU (other threads, other streams) race and must be
+   serialised by the caller.  A failure message, if errbuf is not NULL, is written to errbuf
+   (errlen bytes). */
+int ampcor_correlate_noalloc(const ampcor_params* params, const ampcor_job* job, void* stream,
+                             char* errbuf, size_t errlen);
+
 /* Message of the last failure on handle (or of the last failed ampcor_create when handle is
    NULL). */
 const char* ampcor_last_error(const ampcor_handle* handle);
