@@ -42,6 +42,13 @@ int round_nv(int w)
 }
 
 int odd_at_least(int x) { return (x % 2) ? x : x + 1; }
+
+int ncc_block_width()
+{
+    const char* env = std::getenv("AMPCOR_NCC_BLOCK");
+    if (env && std::atoi(env) == 16) return 16;
+    return 32;
+}
 int round4(int x) { return (x + 3) & ~3; }
 
 // split of one correlation surface over the warps of a CTA and its shared-memory layout;
@@ -57,8 +64,10 @@ bool plan_ncc(int R, int W, int extra_win, int extra_chip, NccGeom& g, std::stri
     g.R = R;
     g.W = W;
     g.C = C;
-    // column blocks: a first block of up to 33 placements, then blocks of 32
-    const int blocks = (C <= 33) ? 1 : 1 + (C - 33 + 31) / 32;
+    // column blocks: a first block of up to bw + 1 placements, then blocks of bw (bw = 32, or 16
+    // with AMPCOR_NCC_BLOCK=16 for a smaller unrolled loop; on B200 both run at the same speed)
+    const int bw = ncc_block_width();
+    const int blocks = (C <= bw + 1) ? 1 : 1 + (C - (bw + 1) + bw - 1) / bw;
     if (blocks > kMaxVB) {
         err = "search margin too large for this build (at most 8 column blocks)";
         return false;
@@ -67,7 +76,7 @@ bool plan_ncc(int R, int W, int extra_win, int extra_chip, NccGeom& g, std::stri
     int v0 = 0;
     int need_s = W, need_cs = R;
     for (int b = 0; b < blocks; ++b) {
-        const int w = (b == 0) ? C - 32 * (blocks - 1) : 32;
+        const int w = (b == 0) ? C - bw * (blocks - 1) : bw;
         const int nv = round_nv(w);
         if (nv < 0) {
             err = "internal: no register block for width " + std::to_string(w);
