@@ -23,6 +23,7 @@ E_NOMEM = 4
 E_BOUNDS = 5
 E_STATE = 6
 FLAG_REF_COMPAT = 1
+FLAG_PLAIN_FP32 = 2
 
 STATUS_NAMES = {
     OK: "AMPCOR_OK",
@@ -99,6 +100,8 @@ SIGNATURES = {
     "ampcor_profile": (c_int, [c_void_p, c_int]),
     "ampcor_stage_times": (c_int, [c_void_p, POINTER(ctypes.c_double), POINTER(ctypes.c_double),
                                    POINTER(ctypes.c_double), POINTER(c_uint64)]),
+    "ampcor_kernel_times": (c_int, [c_void_p, POINTER(ctypes.c_double), POINTER(c_uint64)]),
+    "ampcor_form": (c_int, [c_void_p]),
     "ampcor_correlate_noalloc": (c_int, [POINTER(Params), POINTER(Job), c_void_p, ctypes.c_char_p,
                                          ctypes.c_size_t]),
     "ampcor_last_error": (c_char_p, [c_void_p]),

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CC = "/usr/bin/gcc"
 
-CUDA_SOURCES = ["kernels.cu", "capi.cu"]
+CUDA_SOURCES = ["kernels.cu", "tc_ncc.cu", "capi.cu"]
 CUDA_HEADERS = ["kernels.cuh", os.path.join("..", "..", "include", "ampcor_b200.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

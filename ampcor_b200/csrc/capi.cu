@@ -156,6 +156,65 @@ bool plan_interp(int N, int f, InterpGeom& ig, std::string& err)
     return true;
 }
 
+// the tensor-core form of one surface: needs C <= 128 (the accumulator's 128 lanes hold the
+// placement columns) and C <= 256 accumulator columns
+bool plan_tc(int R, int W, int raw_bytes, TcGeom& g, std::string& err)
+{
+    std::memset(&g, 0, sizeof(g));
+    const int C = W - R + 1;
+    if (C < 1 || C > 128) {
+        err = "the tensor-core form needs at most 128 placements per axis";
+        return false;
+    }
+    g.R = R;
+    g.W = W;
+    g.C = C;
+    g.N = (C + 15) / 16 * 16;
+    g.JC = std::min(64, (R + 15) / 16 * 16);
+    g.nchunks = (R + g.JC - 1) / g.JC;
+    g.Q = W + g.N - 1;
+    g.XR = 128 + g.JC - 8;
+    g.RB = g.XR + 8;
+    g.nst = 4;
+    // the tensor cores truncate when they add into an FP32 accumulator, which shrinks long sums
+    // by a relative amount that grows with the number of additions; spreading the window rows over
+    // several accumulators (summed with round-to-nearest at the end) divides that bias by their
+    // count.  256 columns per CTA keeps two CTAs per SM within the 512 columns of an SM.
+    g.nacc = std::max(1, std::min(8, 256 / g.N));
+    g.tmem_cols = 32;
+    while (g.tmem_cols < g.nacc * g.N) g.tmem_cols *= 2;
+    auto up = [](int x, int a) { return (x + a - 1) / a * a; };
+    int off = 0;
+    g.off_crev = off;
+    off = up(off + 2 * (g.JC / 8) * g.Q * 16, 1024);
+    g.off_x = off;
+    off = up(off + g.nst * 2 * g.XR * 16, 1024);
+    g.off_row = off;
+    off = up(off + g.nst * g.RB * 4, 128);
+    g.off_raw = off;  // kPrefetch raw window rows of RB elements (complex64 or fp32)
+    off = up(off + 8 * g.RB * raw_bytes, 128);
+    g.off_bar = off;
+    off = up(off + (2 * g.nst + 2) * 8, 128);
+    g.off_misc = off;
+    off += 256;
+    g.smem_bytes = off;
+    if (g.Q > 16383 || g.smem_bytes > 227 * 1024) {
+        err = "tile geometry too large for the tensor-core form";
+        return false;
+    }
+    return true;
+}
+
+// shared memory of the statistics kernels: the staged window and the FP64 column-sum chunk
+NccGeom stats_layout(const NccGeom& g)
+{
+    NccGeom s = g;
+    s.off_win = 0;
+    s.off_chip = round4(g.W * g.S);
+    s.smem_bytes = (s.off_chip + 4 * kStatRows * (g.W + 1)) * 4;
+    return s;
+}
+
 // band-limited interpolation kernel of an N-periodic sequence (Nyquist pair halved for even N):
 // the zero-padded inverse FFT with a 1/N scale, written as a sum of cosines
 double dirichlet(int N, double d)
@@ -220,9 +279,22 @@ struct ampcor_handle {
     size_t job_offsets_cap = 0;
     ampcor_pair_diag* d_job_diag = nullptr;
     size_t job_diag_cap = 0;
-    // per-stage timing: (start, stop) event pairs of each kernel launch, per stage
+    // tensor-core form
+    bool tensor = false;
+    TcGeom tcc{}, tcf{};
+    NccGeom gsc{}, gsf{};
+    int zoom_smem = 0;
+    float* d_inv_c = nullptr;
+    float* d_inv_f = nullptr;
+    float* d_gam = nullptr;
+    FineOut* d_fine_out = nullptr;
+    size_t fine_cap = 0;
+    unsigned int* d_tc_err = nullptr;
+    // per-kernel timing: (start, stop) event pairs of each launch, per kernel kind
+    // (0 coarse correlation, 1 refinement, 2 fine correlation, 3 coarse statistics,
+    //  4 fine statistics, 5 zoom)
     bool profiling = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks[3];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks[6];
     std::string err;
 };
 
@@ -311,6 +383,25 @@ int ensure_refined(ampcor_handle* h)
         h->d_refined = nullptr;
         return fail(h, AMPCOR_E_NOMEM, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
     }
+    if (h->tensor) {
+        const size_t n = h->chunk;
+        if (cudaMalloc(&h->d_inv_c, n * h->C * h->C * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&h->d_inv_f, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&h->d_gam, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess)
+            return fail(h, AMPCOR_E_NOMEM, "allocating tensor-core form scratch");
+    }
+    return AMPCOR_OK;
+}
+
+int ensure_fine_out(ampcor_handle* h, size_t pairs)
+{
+    if (h->fine_cap >= pairs && h->d_fine_out) return AMPCOR_OK;
+    cudaFree(h->d_fine_out);
+    h->d_fine_out = nullptr;
+    h->fine_cap = 0;
+    if (cudaMalloc(&h->d_fine_out, std::max<size_t>(pairs, 1) * sizeof(FineOut)) != cudaSuccess)
+        return fail(h, AMPCOR_E_NOMEM, "allocating refined maxima");
+    h->fine_cap = std::max<size_t>(pairs, 1);
     return AMPCOR_OK;
 }
 
@@ -329,9 +420,9 @@ void keep(ampcor_handle* h, int stage, cudaEvent_t a, cudaEvent_t b)
     if (a && b) h->marks[stage].emplace_back(a, b);
 }
 
-// enqueue coarse -> (refine -> fine) per chunk on stream st
-int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
-                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+// plain FP32 form: coarse over all pairs, then (refine -> fine) per chunk on stream st
+int run_plain(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+              PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
 {
     if (pairs == 0) return AMPCOR_OK;
     int rc = ensure_refined(h);
@@ -372,6 +463,58 @@ void drop_marks(ampcor_handle* h)
         v.clear();
     }
     for (cudaEvent_t e : seen) cudaEventDestroy(e);
+}
+
+// tensor-core form, per chunk: coarse statistics -> coarse correlation -> refinement -> fine
+// statistics -> fine correlation -> zoom
+int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+               PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+{
+    if (pairs == 0) return AMPCOR_OK;
+    int rc = ensure_refined(h);
+    if (rc) return rc;
+    if ((rc = ensure_fine_out(h, (size_t)pairs))) return rc;
+    const RealTiles rt{h->d_refined, h->refined_stride, 0, (long long)h->Rf * h->Rf};
+    const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
+    for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
+        const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
+        cudaEvent_t a = mark(h, st);
+        window_stats_cplx_kernel<<<n, kThreads, h->gsc.smem_bytes, st>>>(src, c0, n, h->gsc, h->d_inv_c);
+        cudaEvent_t b = mark(h, st);
+        keep(h, 3, a, b);
+        tc_coarse_kernel<<<n, 256, h->tcc.smem_bytes, st>>>(src, c0, n, h->tcc, h->d_inv_c, h->m,
+                                                            h->d_coarse, h->d_coarse_peak,
+                                                            coarse_surfaces, h->d_tc_err);
+        cudaEvent_t c = mark(h, st);
+        keep(h, 0, b, c);
+        refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
+                                                           h->d_chip_taps, h->d_win_taps,
+                                                           h->d_refined, h->refined_stride);
+        cudaEvent_t d = mark(h, st);
+        keep(h, 1, c, d);
+        window_stats_real_kernel<<<n, kThreads, h->gsf.smem_bytes, st>>>(rt, n, h->gsf, h->d_inv_f);
+        cudaEvent_t e = mark(h, st);
+        keep(h, 4, d, e);
+        tc_fine_kernel<<<n, 256, h->tcf.smem_bytes, st>>>(rt, c0, n, h->tcf, h->d_inv_f, src.ref_off,
+                                                          h->d_fine_out, h->d_gam, refined_surfaces,
+                                                          h->d_tc_err);
+        cudaEvent_t f = mark(h, st);
+        keep(h, 2, e, f);
+        zoom_kernel<<<n, kThreads, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg,
+                                                       h->d_zoom_taps, h->d_coarse, h->d_coarse_peak,
+                                                       h->d_fine_out, h->M, h->f, h->m, compat,
+                                                       offsets, diag);
+        keep(h, 5, f, mark(h, st));
+        CK(h, cudaGetLastError(), "launching the tensor-core pipeline");
+    }
+    return AMPCOR_OK;
+}
+
+int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+{
+    return h->tensor ? run_tensor(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st)
+                     : run_plain(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
 }
 
 cudaStream_t pick(ampcor_handle* h, void* stream)
@@ -440,6 +583,18 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         return create_fail(AMPCOR_E_SHAPE, err);
     }
     h->refine_smem = std::max(h->ic.smem_bytes, h->iw.smem_bytes);
+    // the tensor-core form unless the plain FP32 form is asked for or the geometry needs it
+    {
+        const char* form = std::getenv("AMPCOR_FORM");
+        bool want = !(p->flags & AMPCOR_FLAG_PLAIN_FP32);
+        if (form && std::strcmp(form, "plain") == 0) want = false;
+        if (form && std::strcmp(form, "tensor") == 0) want = true;
+        std::string terr;
+        h->tensor = want && plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
+        h->gsc = stats_layout(h->gc);
+        h->gsf = stats_layout(h->gf);
+        h->zoom_smem = (round4(h->Cf * h->Cf) + round4(h->Cf * h->Z) + round4(h->z * h->zg.taps_len) + 64) * 4;
+    }
 
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) {
@@ -460,6 +615,16 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         (e = cudaFuncSetAttribute(fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(window_stats_cplx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(window_stats_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(tc_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(tc_fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(zoom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kMaxSmem)) != cudaSuccess)
         return cuda_create_fail(e, "configuring kernel shared memory");
 
@@ -476,8 +641,10 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         (e = upload(h->d_zoom_taps, zt)) != cudaSuccess)
         return cuda_create_fail(e, "uploading interpolation taps");
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
-        (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess)
-        return cuda_create_fail(e, "allocating the bounds counter");
+        (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_tc_err, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMemset(h->d_tc_err, 0, sizeof(unsigned int))) != cudaSuccess)
+        return cuda_create_fail(e, "allocating the error counters");
     *out = h;
     return AMPCOR_OK;
 }
@@ -504,6 +671,11 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_ulhc);
     cudaFree(h->d_job_offsets);
     cudaFree(h->d_job_diag);
+    cudaFree(h->d_inv_c);
+    cudaFree(h->d_inv_f);
+    cudaFree(h->d_gam);
+    cudaFree(h->d_fine_out);
+    cudaFree(h->d_tc_err);
     drop_marks(h);
     if (h->h_arena) cudaFreeHost(h->h_arena);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
@@ -627,9 +799,15 @@ int ampcor_synchronize(ampcor_handle* h, void* stream)
     if (!h) return AMPCOR_E_ARG;
     CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
     cudaStream_t st = pick(h, stream);
-    unsigned int bad = 0;
+    unsigned int bad = 0, tcerr = 0;
     CK(h, cudaMemcpyAsync(&bad, h->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, st), "reading the bounds counter");
+    CK(h, cudaMemcpyAsync(&tcerr, h->d_tc_err, sizeof(tcerr), cudaMemcpyDeviceToHost, st), "reading the error counter");
     CK(h, cudaStreamSynchronize(st), "running the correlation pipeline");
+    if (tcerr) {
+        CK(h, cudaMemsetAsync(h->d_tc_err, 0, sizeof(unsigned int), st), "resetting the error counter");
+        CK(h, cudaStreamSynchronize(st), "resetting the error counter");
+        return fail(h, AMPCOR_E_CUDA, std::to_string(tcerr) + " tile pair(s) timed out in the tensor-core pipeline");
+    }
     if (bad) {
         CK(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned int), st), "resetting the bounds counter");
         CK(h, cudaStreamSynchronize(st), "resetting the bounds counter");
@@ -699,9 +877,9 @@ int ampcor_stage_times(ampcor_handle* h, double* coarse_ms, double* refine_ms, d
 {
     if (!h) return AMPCOR_E_ARG;
     CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
-    double t[3] = {0.0, 0.0, 0.0};
+    double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     uint64_t n = 0;
-    for (int s = 0; s < 3; ++s)
+    for (int s = 0; s < 6; ++s)
         for (auto& pr : h->marks[s]) {
             CK(h, cudaEventSynchronize(pr.second), "waiting for a stage event");
             float ms = 0.0f;
@@ -710,11 +888,36 @@ int ampcor_stage_times(ampcor_handle* h, double* coarse_ms, double* refine_ms, d
             ++n;
         }
     drop_marks(h);
-    if (coarse_ms) *coarse_ms = t[0];
+    if (coarse_ms) *coarse_ms = t[0] + t[3];
     if (refine_ms) *refine_ms = t[1];
-    if (fine_ms) *fine_ms = t[2];
+    if (fine_ms) *fine_ms = t[2] + t[4] + t[5];
     if (launches) *launches = n;
     return AMPCOR_OK;
+}
+
+int ampcor_kernel_times(ampcor_handle* h, double* ms, uint64_t* launches)
+{
+    if (!h || !ms || !launches) return fail(h, AMPCOR_E_ARG, "null argument");
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    for (int s = 0; s < 6; ++s) {
+        ms[s] = 0.0;
+        launches[s] = 0;
+        for (auto& pr : h->marks[s]) {
+            CK(h, cudaEventSynchronize(pr.second), "waiting for a kernel event");
+            float x = 0.0f;
+            CK(h, cudaEventElapsedTime(&x, pr.first, pr.second), "reading a kernel event");
+            ms[s] += x;
+            ++launches[s];
+        }
+    }
+    drop_marks(h);
+    return AMPCOR_OK;
+}
+
+int ampcor_form(const ampcor_handle* h)
+{
+    if (!h) return -1;
+    return h->tensor ? 1 : 0;
 }
 
 int ampcor_surface_dims(const ampcor_handle* h, int32_t* coarse, int32_t* refined, int32_t* zoomed)

@@ -699,4 +699,85 @@ fine_kernel(const float* refined, long long refined_stride, long long pair0, lon
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// helpers of the tensor-core form: placement statistics and the zoom, as separate kernels
+// ------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads, 1)
+window_stats_cplx_kernel(PairSource src, long long pair0, long long pairs, NccGeom g, float* inv)
+{
+    extern __shared__ __align__(16) float smem[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    const long long toff = src.tgt_off[p];
+    if (toff < 0 || src.ref_off[p] < 0) return;
+    float* win = smem + g.off_win;
+    stage_cplx(win, g.W, g.W, g.S, src.tgt_base + toff, src.tgt_stride);
+    __syncthreads();
+    window_stats(win, g, inv + (long long)blockIdx.x * g.C * g.C,
+                 reinterpret_cast<double*>(smem + g.off_chip));
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+window_stats_real_kernel(RealTiles t, long long pairs, NccGeom g, float* inv)
+{
+    extern __shared__ __align__(16) float smem[];
+    if (blockIdx.x >= pairs) return;
+    float* win = smem + g.off_win;
+    stage_real(win, g.W, g.W, g.S, t.base + (long long)blockIdx.x * t.stride + t.win_off);
+    __syncthreads();
+    window_stats(win, g, inv + (long long)blockIdx.x * g.C * g.C,
+                 reinterpret_cast<double*>(smem + g.off_chip));
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+zoom_kernel(const float* gam, long long pair0, long long pairs, const long long* ref_off,
+            ZoomGeom zg, const float* zoom_taps, const CoarseOut* coarse, const float* coarse_peak,
+            const FineOut* fout, int margin, int refine_factor, int refine_margin, int ref_compat,
+            float2* offsets, PairDiag* diag)
+{
+    extern __shared__ __align__(16) float smem[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    if (ref_off[p] < 0) {
+        if (threadIdx.x == 0) {
+            offsets[p] = make_float2(NAN, NAN);
+            if (diag) diag[p] = PairDiag{-1, -1, -1, -1, -1, -1, -1, -1, NAN, NAN, NAN, 0.0f};
+        }
+        return;
+    }
+    const int Cf = zg.Cf;
+    float* G = smem;
+    float* T = G + ((Cf * Cf + 3) & ~3);
+    float* taps = T + ((Cf * zg.Z + 3) & ~3);
+    float* red = taps + ((zg.z * zg.taps_len + 3) & ~3);
+    const float* src = gam + (long long)blockIdx.x * Cf * Cf;
+    for (int idx = threadIdx.x; idx < Cf * Cf; idx += kThreads) G[idx] = src[idx];
+    for (int idx = threadIdx.x; idx < zg.z * zg.taps_len; idx += kThreads) taps[idx] = __ldg(zoom_taps + idx);
+    __syncthreads();
+    float zv;
+    int zi;
+    zoom_argmax(G, T, taps, zg, zv, zi);
+    block_argmax(zv, zi, red, reinterpret_cast<int*>(red + kWarps));
+    if (threadIdx.x == 0) {
+        const CoarseOut co = coarse[p];
+        const FineOut fo = fout[p];
+        const int fp = zi / zg.Z, fq = zi - fp * zg.Z;
+        const float zoom = (float)(refine_factor * zg.z);
+        float dy, dx;
+        if (ref_compat) {
+            dy = ((float)co.top - (float)margin) + ((float)fp / zoom - (float)refine_margin);
+            dx = ((float)co.left - (float)margin) + ((float)fq / zoom - (float)refine_margin);
+        } else {
+            dy = (float)(co.top - margin) + (float)fp / zoom;
+            dx = (float)(co.left - margin) + (float)fq / zoom;
+        }
+        offsets[p] = make_float2(dy, dx);
+        if (diag) {
+            diag[p] = PairDiag{co.u, co.v, co.top, co.left, fo.u, fo.v, fp, fq, coarse_peak[p],
+                               fo.peak, zv, 0.0f};
+        }
+    }
+}
+
 }  // namespace ampcor_b200

@@ -92,6 +92,42 @@ struct PairDiag {
     float pad;
 };
 
+// dense fp32 amplitude tiles of a chunk of pairs (the refined tiles): the tile set of chunk-local
+// pair q starts at base + q * stride; the chip (R x R, row stride R) at chip_off and the window
+// (W x W, row stride W) at win_off within it
+struct RealTiles {
+    const float* base;
+    long long stride;
+    long long chip_off;
+    long long win_off;
+};
+
+// the tensor-core form of one correlation surface: D[v][u] = sum_w sum_j A_w[v][j] B_w[j][u]
+// accumulated in tensor memory, A_w[v][j] = t(w, v + j) (window row w, read through overlapping
+// 16-byte rows X[p] = t(w, p .. p+7)), B_w[j][u] = r'(w - u, j) (the zero-mean chip, rows
+// reversed, so that B_w is a window of one fixed buffer that slides by one row per window row)
+struct TcGeom {
+    int R, W, C;
+    int N;          // accumulator columns (placement rows u), multiple of 16, >= C
+    int JC;         // chip columns per pass over the window rows (multiple of 16)
+    int nchunks;    // passes: ceil(R / JC)
+    int Q;          // rows of the reversed-chip buffer: W + N - 1
+    int XR;         // 16-byte rows of one window-row operand: 128 + JC - 8
+    int RB;         // floats of one window-row buffer: XR + 8
+    int nst;        // operand stages in flight
+    int nacc;       // accumulators: window row it goes to accumulator it % nacc
+    int tmem_cols;  // tensor-memory columns allocated (power of two >= nacc N)
+    int off_crev, off_x, off_row, off_raw, off_bar, off_misc;   // shared-memory regions, bytes
+    int smem_bytes;
+};
+
+// refined-surface maximum of one pair
+struct FineOut {
+    int u, v;
+    float peak;
+    float pad;
+};
+
 __global__ void pair_offsets_kernel(const int* ulhc, long long pairs, long long ref_lines,
                                     long long ref_samples, long long tgt_lines,
                                     long long tgt_samples, int R, int W, long long* ref_off,
@@ -114,5 +150,26 @@ __global__ void fine_kernel(const float* refined, long long refined_stride, long
                             const float* coarse_peak, int margin, int refine_factor,
                             int refine_margin, int ref_compat, float2* offsets, PairDiag* diag,
                             float* surfaces);
+
+// FP64 window statistics of every placement, 1/sqrt(sum (t - mu)^2) (0 for a flat box), for the
+// tensor-core form: C^2 floats per chunk-local pair
+__global__ void window_stats_cplx_kernel(PairSource src, long long pair0, long long pairs, NccGeom g,
+                                         float* inv);
+__global__ void window_stats_real_kernel(RealTiles t, long long pairs, NccGeom g, float* inv);
+
+// tensor-core correlation (bf16x3 split products, FP32 accumulation in tensor memory)
+__global__ void tc_coarse_kernel(PairSource src, long long pair0, long long pairs, TcGeom g,
+                                 const float* inv, int m, CoarseOut* out, float* coarse_peak,
+                                 float* surfaces, unsigned int* err);
+__global__ void tc_fine_kernel(RealTiles t, long long pair0, long long pairs, TcGeom g,
+                               const float* inv, const long long* ref_off, FineOut* fout,
+                               float* gam, float* surfaces, unsigned int* err);
+
+// zoom of the refined surfaces of a chunk (C^2 floats per chunk-local pair), offsets
+__global__ void zoom_kernel(const float* gam, long long pair0, long long pairs,
+                            const long long* ref_off, ZoomGeom zg, const float* zoom_taps,
+                            const CoarseOut* coarse, const float* coarse_peak, const FineOut* fout,
+                            int margin, int refine_factor, int refine_margin, int ref_compat,
+                            float2* offsets, PairDiag* diag);
 
 }  // namespace ampcor_b200

@@ -36,7 +36,7 @@ class Worker:
     """A correlator bound to one CUDA device."""
 
     def __init__(self, pairs, chip, window, refine_factor=2, refine_margin=8, zoom_factor=4,
-                 device=0, ref_compat=False):
+                 device=0, ref_compat=False, plain=False):
         self._lib = _lib.load()
         chip = tuple(int(c) for c in chip)
         window = tuple(int(w) for w in window)
@@ -57,7 +57,7 @@ class Worker:
             refine_margin=self.refine_margin,
             zoom_factor=self.zoom_factor,
             device=self.device,
-            flags=_lib.FLAG_REF_COMPAT if ref_compat else 0,
+            flags=(_lib.FLAG_REF_COMPAT if ref_compat else 0) | (_lib.FLAG_PLAIN_FP32 if plain else 0),
         )
         handle = c_void_p()
         _check(self._lib, None, self._lib.ampcor_create(byref(params), byref(handle)))
@@ -65,6 +65,8 @@ class Worker:
         c, r, z = c_int32(), c_int32(), c_int32()
         self._lib.ampcor_surface_dims(handle, byref(c), byref(r), byref(z))
         self.coarse_dim, self.refined_dim, self.zoomed_dim = c.value, r.value, z.value
+        # "tensor": bf16x3 split products on the tensor cores; "plain": FP32 FMA
+        self.form = "tensor" if self._lib.ampcor_form(handle) == 1 else "plain"
 
     # lifetime
     def close(self):
@@ -126,6 +128,16 @@ class Worker:
         _check(self._lib, self._handle,
                self._lib.ampcor_stage_times(self._handle, byref(c), byref(r), byref(f), byref(n)))
         return c.value, r.value, f.value, n.value
+
+    KERNELS = ("coarse_correlation", "refinement", "fine_correlation", "coarse_statistics",
+               "fine_statistics", "zoom")
+
+    def kernel_times(self):
+        """{kernel: (ms, launches)} since profiling started or was last read."""
+        ms = (ctypes.c_double * 6)()
+        n = (ctypes.c_uint64 * 6)()
+        _check(self._lib, self._handle, self._lib.ampcor_kernel_times(self._handle, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 
     # whole rasters
     def correlate(self, ref, tgt, ulhc, offsets=None, diag=None, coarse_surfaces=None,

@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--plain", action="store_true",
+                    help="plain FP32 form instead of the tensor-core form")
     ap.add_argument("--pairs", type=int, default=0,
                     help="correlate only the first N pairs (small cases for profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -221,7 +223,7 @@ def run_b200(args):
         w.truth = None if w.truth is None else w.truth[: args.pairs]
     worker = Worker(pairs=w.pairs, chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
-                    zoom_factor=w.zoom_factor, device=local)
+                    zoom_factor=w.zoom_factor, device=local, plain=args.plain)
     ref = torch.from_numpy(w.ref).to(dev)
     tgt = torch.from_numpy(w.tgt).to(dev)
     ulhc = torch.from_numpy(w.ulhc).to(dev)
@@ -251,7 +253,8 @@ def run_b200(args):
     torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
-    coarse_ms, refine_ms, fine_ms, launches = worker.stage_times()
+    kt = worker.kernel_times()
+    launches = sum(n for _, n in kt.values())
     worker.profile(False)
     clk = clocks.stop()
     # result check outside the timed region
@@ -289,24 +292,31 @@ def run_b200(args):
 
     line = None
     if rank == 0:
-        per_launch_pairs_fine = min(worker_chunk(), w.pairs)
-        n_chunks = -(-w.pairs // per_launch_pairs_fine)
         C = w.window - w.chip + 1
+        E = w.chip + 2 * w.refine_margin
         Rf = w.refine_factor * w.chip
         Cf = 2 * w.refine_factor * w.refine_margin + 1
-        flop_coarse = 2.0 * w.chip ** 2 * C ** 2
-        flop_fine = 2.0 * Rf ** 2 * Cf ** 2
-        stage = {"coarse_kernel": coarse_ms, "refine_kernel": refine_ms, "fine_kernel": fine_ms}
-        top = max(stage, key=stage.get)
-        if top == "coarse_kernel":
-            per_launch_ms = coarse_ms / args.steps
-            flops = flop_coarse * w.pairs
-        elif top == "fine_kernel":
-            per_launch_ms = fine_ms / (args.steps * n_chunks)
-            flops = flop_fine * per_launch_pairs_fine
-        else:
-            per_launch_ms = refine_ms / (args.steps * n_chunks)
-            flops = flop_fine * per_launch_pairs_fine  # not a contraction; reported for scale
+        f = w.refine_factor
+        # algorithmic flops per pair of each kernel kind (direct-form numerators; the
+        # refinement's separable interpolation)
+        flop_pair = {
+            "coarse_correlation": 2.0 * w.chip ** 2 * C ** 2,
+            "fine_correlation": 2.0 * Rf ** 2 * Cf ** 2,
+            "refinement": 4.0 * (f * f - 1) * (w.chip ** 3 + E ** 3),
+        }
+        names = {
+            "coarse_correlation": "tc_coarse_kernel" if worker.form == "tensor" else "coarse_kernel",
+            "fine_correlation": "tc_fine_kernel" if worker.form == "tensor" else "fine_kernel",
+            "refinement": "refine_kernel",
+            "coarse_statistics": "window_stats_cplx_kernel",
+            "fine_statistics": "window_stats_real_kernel",
+            "zoom": "zoom_kernel",
+        }
+        top = max(flop_pair, key=lambda k: kt[k][0])
+        top_ms, top_n = kt[top]
+        per_launch_ms = top_ms / max(top_n, 1)
+        pairs_per_launch = w.pairs * args.steps / max(top_n, 1)
+        flops = flop_pair[top] * pairs_per_launch
         achieved = flops / (per_launch_ms / 1000.0) / 1e12
         peaks = {}
         try:
@@ -317,11 +327,8 @@ def run_b200(args):
         peak_src = "of measured" if tensor_peak else "of fallback"
         tensor_peak = tensor_peak or 1590.0
         simt = fp32_peak(local)
-        traffic = load_traffic().get(top)
-        traffic_per_launch = None
-        if traffic:
-            units = w.pairs if top == "coarse_kernel" else per_launch_pairs_fine
-            traffic_per_launch = traffic["bytes_per_pair"] * units
+        traffic = load_traffic().get(names[top])
+        traffic_per_launch = traffic["bytes_per_pair"] * pairs_per_launch if traffic else None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -335,16 +342,20 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": workload_config(w),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3" if worker.form == "tensor" else "f32",
+            "data": "synthetic", "config": dict(workload_config(w), form=worker.form),
             "roofline": {
-                "bound": "tensor", "kernel": top, "achieved": achieved, "peak": tensor_peak,
-                "unit": "TFLOP/s", "frac": achieved / tensor_peak, "traffic": traffic_per_launch,
+                "bound": "tensor", "kernel": names[top], "achieved": achieved,
+                "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved / tensor_peak,
+                "traffic": traffic_per_launch,
                 "peak_note": (f"dense bf16 tensor peak {peak_src} (MEASURED_PEAKS.json burst); "
-                              f"the plain form runs on the FP32 pipes"),
+                              f"achieved counts the algorithmic flops of the direct-form "
+                              f"numerator only"),
                 "fp32_simt_peak": simt, "fp32_simt_frac": achieved / simt if simt > 0 else None,
                 "algorithmic_flop_per_launch": flops, "ms_per_launch": per_launch_ms,
-                "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
+                "kernel_ms_per_step": {names[k]: v[0] / args.steps for k, v in kt.items() if v[1]},
+                "launches_per_step": {names[k]: v[1] / args.steps for k, v in kt.items() if v[1]},
             },
             "e2e": ({"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                      "d2h_bytes_per_step": d2h, "steps": e2e_steps} if e2e_value else None),

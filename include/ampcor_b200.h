@@ -31,6 +31,8 @@ extern "C" {
 #define AMPCOR_FLAG_REF_COMPAT 1u  /* assemble offsets with the reference formula, which
                                       subtracts the refine margin a second time
                                       (lib/libampcor_cuda/correlators/offsets.cu:124-125) */
+#define AMPCOR_FLAG_PLAIN_FP32 2u  /* correlate with FP32 fused multiply-adds (the plain form)
+                                      instead of bf16x3 split products on the tensor cores */
 
 typedef struct ampcor_handle ampcor_handle;
 
@@ -166,6 +168,18 @@ int ampcor_stage_times(ampcor_handle* handle, double* coarse_ms, double* refine_
    (errlen bytes). */
 int ampcor_correlate_noalloc(const ampcor_params* params, const ampcor_job* job, void* stream,
                              char* errbuf, size_t errlen);
+
+/* Device time (ms) and launch count per kernel kind since profiling was switched on or last read:
+   [0] coarse correlation, [1] refinement, [2] fine correlation, [3] coarse placement statistics,
+   [4] fine placement statistics, [5] zoom ([3]-[5] run in the tensor-core form only); resets the
+   counters.  No reference counterpart. */
+int ampcor_kernel_times(ampcor_handle* handle, double* ms, uint64_t* launches);
+
+/* 1 if the worker correlates on the tensor cores (bf16x3 split products), 0 for the plain FP32
+   form, -1 for a NULL handle.  The tensor-core form is the default wherever the geometry allows
+   it (at most 128 placements per axis); AMPCOR_FLAG_PLAIN_FP32 selects the plain form.  No
+   reference counterpart. */
+int ampcor_form(const ampcor_handle* handle);
 
 /* Message of the last failure on handle (or of the last failed ampcor_create when handle is
    NULL). */

@@ -27,11 +27,15 @@ PEAK_RTOL = 1e-5
 SURF_ATOL = 2e-5
 
 
-def run_device(w: synth.Workload, ulhc=None, surfaces=False):
+FORMS = ["tensor", "plain"]
+
+
+def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor"):
     ulhc = w.ulhc if ulhc is None else ulhc
     worker = Worker(pairs=len(ulhc), chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
-                    zoom_factor=w.zoom_factor)
+                    zoom_factor=w.zoom_factor, plain=(form == "plain"))
+    assert worker.form == form
     dev = torch.device("cuda:0")
     ref = torch.from_numpy(w.ref).to(dev)
     tgt = torch.from_numpy(w.tgt).to(dev)
@@ -84,9 +88,10 @@ def check_parity(w, ulhc, gpu, label):
     return off, od
 
 
-def test_plain_512_parity():
+@pytest.mark.parametrize("form", FORMS)
+def test_plain_512_parity(form):
     w = synth.plain_512()
-    gpu = run_device(w, surfaces=True)
+    gpu = run_device(w, surfaces=True, form=form)
     off, od, cs, rs = oracle.adjust(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4, surfaces=True)
     check_parity(w, w.ulhc, gpu, "plain_512")
     assert np.all(gpu["offsets"] == np.float32([3.375, -2.75]))
@@ -94,24 +99,26 @@ def test_plain_512_parity():
     np.testing.assert_allclose(gpu["refined"], rs, atol=SURF_ATOL, rtol=0)
 
 
-def test_golden_plain_512_on_gpu():
+@pytest.mark.parametrize("form", FORMS)
+def test_golden_plain_512_on_gpu(form):
     import os
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "plain_512.npz"))
-    gpu = run_device(synth.plain_512())
+    gpu = run_device(synth.plain_512(), form=form)
     assert np.array_equal(gpu["offsets"], g["offsets"])
     assert np.array_equal(gpu["diag"]["coarse_u"], g["coarse_cpu_argmax"][:, 0])
     assert np.array_equal(gpu["diag"]["coarse_v"], g["coarse_cpu_argmax"][:, 1])
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("R,M", [(32, 8), (64, 32)])
-def test_placement_identity(R, M):
+def test_placement_identity(R, M, form):
     # correlate.cc:279-303 (gamma = 1 at the placement, 10 eps_f in FP32 there; FP32 sums of
     # R^2 terms here, so 1e-5), maxcor.cc:296-312 (argmax = placement), nudge.cc:204-225
     ref, tgt, ulhc = placement_identity(R, M, seed=5)
     W, C = R + 2 * M, 2 * M + 1
     w = synth.Workload("identity", ref, tgt, ulhc, np.zeros((len(ulhc), 2)), R, M, 2,
                        min(4, M), 4, None)
-    gpu = run_device(w, surfaces=True)
+    gpu = run_device(w, surfaces=True, form=form)
     d = gpu["diag"]
     i, j = np.divmod(np.arange(C * C), C)
     assert np.array_equal(d["coarse_u"], i) and np.array_equal(d["coarse_v"], j)
@@ -127,33 +134,36 @@ def _subset(w, n, seed=0):
     return idx
 
 
-def test_production_subset_parity():
+@pytest.mark.parametrize("form", FORMS)
+def test_production_subset_parity(form):
     w = synth.production_4096()
     idx = _subset(w, 192)
-    gpu = run_device(w, ulhc=w.ulhc[idx])
+    gpu = run_device(w, ulhc=w.ulhc[idx], form=form)
     check_parity(w, w.ulhc[idx], gpu, "production_4096")
 
 
-def test_heavy_tail_subset_parity():
+@pytest.mark.parametrize("form", FORMS)
+def test_heavy_tail_subset_parity(form):
     w = synth.production_4096(heavy_tail=True)
     idx = _subset(w, 128, seed=1)
-    gpu = run_device(w, ulhc=w.ulhc[idx])
+    gpu = run_device(w, ulhc=w.ulhc[idx], form=form)
     check_parity(w, w.ulhc[idx], gpu, "heavy_tail_4096")
 
 
-def test_production_full_size_properties():
+@pytest.mark.parametrize("form", FORMS)
+def test_production_full_size_properties(form):
     # all 14,400 pairs: finite, near the applied field, and each result identical whether the
     # pair runs in the full batch or in a small one (no cross-pair dependence)
     w = synth.production_4096()
-    full = run_device(w)
+    full = run_device(w, form=form)
     assert np.isfinite(full["offsets"]).all()
     err = np.abs(full["offsets"] - w.truth)
     assert np.quantile(err, 0.99) < 0.2
     idx = _subset(w, 300, seed=2)
-    part = run_device(w, ulhc=w.ulhc[idx])
+    part = run_device(w, ulhc=w.ulhc[idx], form=form)
     assert np.array_equal(part["offsets"], full["offsets"][idx])
     assert np.array_equal(part["diag"], full["diag"][idx])
-    again = run_device(w)
+    again = run_device(w, form=form)
     assert np.array_equal(again["offsets"], full["offsets"])
 
 
@@ -206,3 +216,15 @@ def test_out_of_bounds_pair_reports_and_is_nan():
     torch.cuda.synchronize()
     o = off.cpu().numpy()
     assert np.isnan(o[2]).all() and np.isfinite(o[[0, 1, 3]]).all()
+
+
+def test_tensor_and_plain_forms_agree():
+    # the two forms on the same pairs: same integer and sub-pixel cells except near-ties,
+    # surfaces within the parity tolerance of each other
+    w = synth.production_4096()
+    idx = _subset(w, 256, seed=3)
+    t = run_device(w, ulhc=w.ulhc[idx], surfaces=True, form="tensor")
+    p = run_device(w, ulhc=w.ulhc[idx], surfaces=True, form="plain")
+    np.testing.assert_allclose(t["coarse"], p["coarse"], atol=SURF_ATOL, rtol=0)
+    np.testing.assert_allclose(t["refined"], p["refined"], atol=SURF_ATOL, rtol=0)
+    assert (t["offsets"] == p["offsets"]).all(axis=1).mean() > 0.98

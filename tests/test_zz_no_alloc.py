@@ -51,9 +51,10 @@ def run_noalloc(w, ulhc):
 
 
 def run_regular(w, ulhc):
+    # the allocation-free path runs the plain FP32 kernels: compare with the same form
     worker = Worker(pairs=len(ulhc), chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
-                    zoom_factor=w.zoom_factor)
+                    zoom_factor=w.zoom_factor, plain=True)
     ref, tgt, u = device_batch(w, ulhc)
     diag = torch.zeros((len(ulhc), DIAG_DTYPE.itemsize), dtype=torch.uint8, device=ref.device)
     off = worker.correlate(ref, tgt, u, diag=diag)
