@@ -101,6 +101,7 @@ bool plan_ncc(int R, int W, int extra_win, int extra_chip, NccGeom& g, std::stri
     g.n_kc = g.n_ub ? std::min(R, std::max(1, kWarps / (g.n_ub * g.n_vb))) : 0;
     g.n_main = g.n_ub * g.n_vb * g.n_kc;
     g.n_tkc = (R + 31) / 32;
+    g.stat_rows = kStatRows;
     g.n_trans = (C - 32 * g.n_ub) * g.n_vb * g.n_tkc;
 
     const int win_f = std::max({W * g.S, g.n_main * 32 * kSlot, extra_win});
@@ -169,13 +170,14 @@ bool plan_tc(int R, int W, int raw_bytes, TcGeom& g, std::string& err)
     g.R = R;
     g.W = W;
     g.C = C;
+    g.M = C <= 64 ? 64 : 128;
     g.N = (C + 15) / 16 * 16;
     g.JC = std::min(64, (R + 15) / 16 * 16);
     g.nchunks = (R + g.JC - 1) / g.JC;
     g.Q = W + g.N - 1;
-    g.XR = 128 + g.JC - 8;
+    g.XR = g.M + g.JC - 8;
     g.RB = g.XR + 8;
-    g.nst = 4;
+    g.nst = 3;  // stages of 2 window rows each
     // the tensor cores truncate when they add into an FP32 accumulator, which shrinks long sums
     // by a relative amount that grows with the number of additions; spreading the window rows over
     // several accumulators (summed with round-to-nearest at the end) divides that bias by their
@@ -187,12 +189,13 @@ bool plan_tc(int R, int W, int raw_bytes, TcGeom& g, std::string& err)
     int off = 0;
     g.off_crev = off;
     off = up(off + 2 * (g.JC / 8) * g.Q * 16, 1024);
+    const int rows_per_stage = 2, prefetch = 2 * rows_per_stage;
     g.off_x = off;
-    off = up(off + g.nst * 2 * g.XR * 16, 1024);
+    off = up(off + g.nst * rows_per_stage * 2 * g.XR * 16, 1024);
     g.off_row = off;
-    off = up(off + g.nst * g.RB * 4, 128);
-    g.off_raw = off;  // kPrefetch raw window rows of RB elements (complex64 or fp32)
-    off = up(off + 8 * g.RB * raw_bytes, 128);
+    off = up(off + g.nst * rows_per_stage * g.RB * 4, 128);
+    g.off_raw = off;  // raw window rows in flight, RB elements each (complex64 or fp32)
+    off = up(off + prefetch * g.RB * raw_bytes, 128);
     g.off_bar = off;
     off = up(off + (2 * g.nst + 2) * 8, 128);
     g.off_misc = off;
@@ -206,12 +209,17 @@ bool plan_tc(int R, int W, int raw_bytes, TcGeom& g, std::string& err)
 }
 
 // shared memory of the statistics kernels: the staged window and the FP64 column-sum chunk
+// (unpadded window rows: the statistics walk columns, one thread per column; the chunk of
+// column sums shrinks until two CTAs fit on an SM)
 NccGeom stats_layout(const NccGeom& g)
 {
     NccGeom s = g;
+    s.S = g.W;
     s.off_win = 0;
-    s.off_chip = round4(g.W * g.S);
-    s.smem_bytes = (s.off_chip + 4 * kStatRows * (g.W + 1)) * 4;
+    s.off_chip = round4(g.W * g.W);
+    s.stat_rows = kStatRows;
+    while (s.stat_rows > 1 && (s.off_chip + 4 * s.stat_rows * (g.W + 1)) * 4 > 110 * 1024) s.stat_rows /= 2;
+    s.smem_bytes = (s.off_chip + 4 * s.stat_rows * (g.W + 1)) * 4;
     return s;
 }
 

@@ -196,8 +196,9 @@ __device__ void window_stats(const float* win, const NccGeom& g, float* inv, dou
 {
     const int W = g.W, R = g.R, C = g.C, S = g.S;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int SR = g.stat_rows;
     double* V1 = vbuf;
-    double* V2 = vbuf + kStatRows * (W + 1);
+    double* V2 = vbuf + SR * (W + 1);
     double s1 = 0.0, s2 = 0.0;
     if (tid < W) {
         for (int i = 0; i < R; ++i) {
@@ -207,8 +208,8 @@ __device__ void window_stats(const float* win, const NccGeom& g, float* inv, dou
         }
     }
     const double cells = (double)R * (double)R;
-    for (int u0 = 0; u0 < C; u0 += kStatRows) {
-        const int nrows = min(kStatRows, C - u0);
+    for (int u0 = 0; u0 < C; u0 += SR) {
+        const int nrows = min(SR, C - u0);
         if (tid < W) {
             for (int r = 0; r < nrows; ++r) {
                 const int u = u0 + r;
@@ -703,7 +704,7 @@ fine_kernel(const float* refined, long long refined_stride, long long pair0, lon
 // helpers of the tensor-core form: placement statistics and the zoom, as separate kernels
 // ------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 window_stats_cplx_kernel(PairSource src, long long pair0, long long pairs, NccGeom g, float* inv)
 {
     extern __shared__ __align__(16) float smem[];
@@ -718,7 +719,7 @@ window_stats_cplx_kernel(PairSource src, long long pair0, long long pairs, NccGe
                  reinterpret_cast<double*>(smem + g.off_chip));
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 window_stats_real_kernel(RealTiles t, long long pairs, NccGeom g, float* inv)
 {
     extern __shared__ __align__(16) float smem[];
@@ -730,7 +731,7 @@ window_stats_real_kernel(RealTiles t, long long pairs, NccGeom g, float* inv)
                  reinterpret_cast<double*>(smem + g.off_chip));
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 zoom_kernel(const float* gam, long long pair0, long long pairs, const long long* ref_off,
             ZoomGeom zg, const float* zoom_taps, const CoarseOut* coarse, const float* coarse_peak,
             const FineOut* fout, int margin, int refine_factor, int refine_margin, int ref_compat,

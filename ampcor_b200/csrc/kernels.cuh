@@ -42,6 +42,7 @@ struct NccGeom {
     int vb_w[kMaxVB];      // placement columns in the block
     int vb_nv[kMaxVB];     // register block width (>= vb_w, one of the compiled widths)
     int vb_steps[kMaxVB];  // ceil(R / nv): chip columns are zero-padded to steps * nv
+    int stat_rows;  // placement rows per window-statistics chunk (<= kStatRows)
     // shared-memory regions, in floats from the start of the dynamic buffer
     int off_win, off_part, off_chip, off_inv, off_gam, off_trans, off_red, off_aux;
     int smem_bytes;
@@ -108,11 +109,12 @@ struct RealTiles {
 // reversed, so that B_w is a window of one fixed buffer that slides by one row per window row)
 struct TcGeom {
     int R, W, C;
+    int M;          // accumulator lanes used (placement columns v): 64 when C <= 64, else 128
     int N;          // accumulator columns (placement rows u), multiple of 16, >= C
     int JC;         // chip columns per pass over the window rows (multiple of 16)
     int nchunks;    // passes: ceil(R / JC)
     int Q;          // rows of the reversed-chip buffer: W + N - 1
-    int XR;         // 16-byte rows of one window-row operand: 128 + JC - 8
+    int XR;         // 16-byte rows of one window-row operand: M + JC - 8
     int RB;         // floats of one window-row buffer: XR + 8
     int nst;        // operand stages in flight
     int nacc;       // accumulators: window row it goes to accumulator it % nacc

@@ -8,7 +8,7 @@
 // over w and over the chip columns j:
 //     D[v][u] = sum_w sum_j A_w[v][j] B_w[j][u],   A_w[v][j] = t(w, v + j),
 //                                                  B_w[j][u] = r'(w - u, j)  (0 outside the chip),
-// so D[v][u] = N(u, v) collects in one tensor-memory accumulator (M = 128 lanes for v, N >= C
+// so D[v][u] = N(u, v) collects in tensor memory (M = 64 or 128 accumulator rows for v, N >= C
 // columns for u) with no per-placement bookkeeping.  Both operands are read by the tensor core
 // through K-major shared-memory descriptors without building the Hankel or sheared matrices:
 //   * A_w: window row w is written once as overlapping 16-byte rows X[p] = t(w, p .. p+7); row v
@@ -21,9 +21,10 @@
 // accumulate in FP32, a relative error near 2^-16 per product, below the FP32 summation error of
 // the plain form on these surfaces.
 //
-// A CTA of 256 threads owns one pair: warps 4-7 stream the window rows into a ring of operand
-// stages, lane 0 of warp 0 issues the MMAs and commits each stage back to its producers, warps 0-3
-// read the accumulator and reduce the normalised surface to its first maximum.  Every wait on an
+// A CTA of 256 threads owns one pair: warps 1-7 stream the window rows, two per stage, into a
+// ring of operand stages, lane 0 of warp 0 issues the MMAs and commits each stage back to its
+// producers, warps 0-3 read the accumulators and reduce the normalised surface to its first
+// maximum.  Every wait on an
 // mbarrier is bounded in time; on expiry the kernel records an error, drains the MMAs it issued
 // and frees its tensor memory before returning.
 #include "kernels.cuh"
@@ -39,9 +40,8 @@ namespace {
 
 constexpr int kTcThreads = 256;
 constexpr int kTcWarps = kTcThreads / 32;
-constexpr int kProducerWarp0 = 4;
-constexpr int kProducers = 128;
-constexpr int kM = 128;                      // accumulator lanes = placement columns v
+constexpr int kProducers = 224;               // warps 1-7 stream the window rows
+constexpr int kRowsPerStage = 2;             // window rows per operand stage
 constexpr long long kSpinCycles = 1ll << 31;  // bound of every wait (about a second)
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -155,10 +155,10 @@ __device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr, uint32_t lead, ui
            ((uint64_t)((stride >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// instruction descriptor: bf16 A and B, both K-major, FP32 accumulator, M = 128, N columns
-__device__ __forceinline__ uint32_t instr_desc(int n)
+// instruction descriptor: bf16 A and B, both K-major, FP32 accumulator, M x N
+__device__ __forceinline__ uint32_t instr_desc(int m, int n)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ float amp_of(float2 z)
@@ -272,7 +272,7 @@ struct DenseTiles {
     __device__ static float amp(const Raw& r) { return r; }
 };
 
-constexpr int kPrefetch = 8;  // window rows fetched ahead of the producers
+constexpr int kPrefetch = 2 * kRowsPerStage;  // window rows fetched ahead of the producers
 
 struct SurfaceMax {
     float v;
@@ -320,7 +320,7 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = g.R, W = g.W, C = g.C, Q = g.Q, KH = g.JC / 8, XR = g.XR;
-    const uint32_t xstage_bytes = 2u * XR * 16u;
+    const uint32_t xstage_bytes = (uint32_t)kRowsPerStage * 2u * XR * 16u;
 
     if (tid == 0) {
         *err = 0;
@@ -353,10 +353,11 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
     s2 = block_sum(s2, red);
     const float inv_sigma = s2 > 0.0 ? (float)(1.0 / sqrt(s2)) : 0.0f;
 
-    const uint32_t idesc = instr_desc(g.N);
+    const uint32_t idesc = instr_desc(g.M, g.N);
     const uint32_t crev_addr = saddr(crev);
     const uint32_t x_addr = saddr(xst);
-    int it = 0;  // window rows streamed so far, over all passes
+    const int NR = kRowsPerStage;
+    const int nsi = (W + NR - 1) / NR;  // stages per pass
     for (int jc = 0; jc < g.nchunks; ++jc) {
         // the previous pass must have finished reading the reversed chip before it is rebuilt
         if (jc > 0) mbar_wait(crev_free, (uint32_t)((jc - 1) & 1), err);
@@ -378,10 +379,10 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
         fence_async_smem();
         __syncthreads();
 
-        if (warp >= kProducerWarp0) {
-            // producers: window row w -> overlapping 16-byte rows of this pass's columns.  The
-            // raw rows w + 1 .. w + kPrefetch are in flight (cp.async) while row w is converted.
-            const int pt = tid - kProducerWarp0 * 32;
+        if (warp >= 1) {
+            // producers (warps 1-7): kRowsPerStage window rows per stage -> overlapping 16-byte
+            // rows of this pass's columns.  Raw rows are fetched kPrefetch rows ahead (cp.async).
+            const int pt = tid - 32;
             using Raw = typename Tiles::Raw;
             Raw* raw = reinterpret_cast<Raw*>(tsm + g.off_raw);
             const int ncols = min(g.RB, W - jc * g.JC);  // columns of this pass inside the window
@@ -393,65 +394,76 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
                 cp_async_commit();
             };
             for (int k = 0; k < kPrefetch; ++k) fetch_row(k);
-            for (int w = 0; w < W; ++w, ++it) {
+            for (int si = 0; si < nsi; ++si) {
+                const int it = jc * nsi + si;  // stage sequence number over all passes
                 const int s = it % g.nst;
-                // one producer waits for the stage; the named barrier hands the verdict to all
-                // 128 (every producer leaves the loop together, so the barrier never strands one)
+                // one producer waits for the stage; the named barrier hands the verdict to every
+                // producer (all leave the loop together, so the barrier never strands one)
                 if (pt == 0)
                     *stop = (it >= g.nst && !mbar_wait(&empty[s], (uint32_t)(((it / g.nst) & 1) ^ 1), err)) ? 1 : 0;
-                cp_async_wait<kPrefetch - 1>();
-                asm volatile("bar.sync 1, 128;" ::: "memory");
+                cp_async_wait<kPrefetch - kRowsPerStage>();
+                asm volatile("bar.sync 1, %0;" ::"n"(kProducers) : "memory");
                 if (*stop) break;
-                float* rb = rowbuf + s * g.RB;
-                const Raw* rr = raw + (w % kPrefetch) * g.RB;
-                for (int x = pt; x < g.RB; x += kProducers) rb[x] = x < ncols ? Tiles::amp(rr[x]) : 0.0f;
-                asm volatile("bar.sync 1, 128;" ::: "memory");
-                fetch_row(w + kPrefetch);
+                float* rb = rowbuf + s * NR * g.RB;
+                for (int idx = pt; idx < NR * g.RB; idx += kProducers) {
+                    const int k = idx / g.RB, x = idx - k * g.RB;
+                    const int w = si * NR + k;
+                    rb[idx] = (w < W && x < ncols) ? Tiles::amp(raw[(w % kPrefetch) * g.RB + x]) : 0.0f;
+                }
+                asm volatile("bar.sync 1, %0;" ::"n"(kProducers) : "memory");
+                for (int k = 0; k < NR; ++k) fetch_row((si + 1) * NR + kPrefetch - NR + k);
                 uint4* xs = reinterpret_cast<uint4*>(xst + s * xstage_bytes);
-                for (int p = pt; p < XR; p += kProducers) {
+                for (int idx = pt; idx < NR * XR; idx += kProducers) {
+                    const int k = idx / XR, p = idx - k * XR;
+                    const float* rr = rb + k * g.RB + p;
                     float x[8];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) x[c] = rb[p + c];
+                    for (int c = 0; c < 8; ++c) x[c] = rr[c];
                     uint4 hi, lo;
                     split8(x, hi, lo);
-                    xs[p] = hi;
-                    xs[XR + p] = lo;
+                    xs[(2 * k) * XR + p] = hi;
+                    xs[(2 * k + 1) * XR + p] = lo;
                 }
                 fence_async_smem();
                 mbar_arrive(&full[s]);
             }
             cp_async_wait<0>();
-        } else if (warp == 0) {
-            if (lane == 0) {
-                for (int w = 0; w < W; ++w, ++it) {
-                    const int s = it % g.nst;
-                    if (!mbar_wait(&full[s], (uint32_t)((it / g.nst) & 1), err)) break;
-                    tc_fence_after();
-                    const uint32_t dacc = tmem + (uint32_t)((it % g.nacc) * g.N);
-                    const uint32_t xa = x_addr + s * xstage_bytes;
-                    for (int ks = 0; ks < g.JC / 16; ++ks) {
-                        // A: rows v of X starting at row 16 ks; B: reversed chip from row W-1-w
-                        const uint32_t a_hi = xa + (uint32_t)(16 * ks) * 16u;
-                        const uint32_t a_lo = a_hi + (uint32_t)XR * 16u;
-                        const uint32_t b_hi = crev_addr + (uint32_t)((0 * KH + 2 * ks) * Q + (W - 1 - w)) * 16u;
-                        const uint32_t b_lo = crev_addr + (uint32_t)((1 * KH + 2 * ks) * Q + (W - 1 - w)) * 16u;
-                        const uint64_t da_hi = kmajor_desc(a_hi, 128u, 128u);
-                        const uint64_t da_lo = kmajor_desc(a_lo, 128u, 128u);
-                        const uint64_t db_hi = kmajor_desc(b_hi, (uint32_t)Q * 16u, 128u);
-                        const uint64_t db_lo = kmajor_desc(b_lo, (uint32_t)Q * 16u, 128u);
-                        const uint32_t first = (it < g.nacc && ks == 0) ? 0u : 1u;
-                        mma_bf16(dacc, da_hi, db_hi, idesc, first);
-                        mma_bf16(dacc, da_hi, db_lo, idesc, 1u);
-                        mma_bf16(dacc, da_lo, db_hi, idesc, 1u);
+        } else if (lane == 0) {
+            // warp 0, lane 0: the MMA issuer.  Descriptors advance by plain additions: the start
+            // address sits in the low 14 bits in 16-byte units and never carries out of them.
+            const uint64_t a0 = kmajor_desc(x_addr, 128u, 128u);
+            const uint64_t b0 = kmajor_desc(crev_addr + (uint32_t)(W - 1) * 16u, (uint32_t)Q * 16u, 128u);
+            const uint64_t b_lo_off = (uint64_t)(KH * Q);        // hi -> lo plane of the chip
+            const uint64_t b_ks_off = (uint64_t)(2 * Q);         // next 16 chip columns
+            const uint64_t a_lo_off = (uint64_t)XR;              // hi -> lo rows of a window row
+            int acc_slot = (jc * W) % g.nacc;
+            int row = jc * W;
+            for (int si = 0; si < nsi; ++si) {
+                const int it = jc * nsi + si;
+                const int s = it % g.nst;
+                if (!mbar_wait(&full[s], (uint32_t)((it / g.nst) & 1), err)) break;
+                tc_fence_after();
+                uint64_t as = a0 + (uint64_t)(s * (xstage_bytes >> 4));
+                for (int k = 0; k < NR; ++k, ++row, as += 2 * a_lo_off) {
+                    const int w = si * NR + k;
+                    if (w >= W) break;
+                    const uint32_t dacc = tmem + (uint32_t)(acc_slot * g.N);
+                    const uint32_t keep = row < g.nacc ? 0u : 1u;
+                    if (++acc_slot == g.nacc) acc_slot = 0;
+                    uint64_t a = as;
+                    uint64_t b = b0 - (uint64_t)w;  // reversed chip from row W-1-w
+#pragma unroll 4
+                    for (int ks = 0; ks < g.JC / 16; ++ks, a += 16, b += b_ks_off) {
+                        mma_bf16(dacc, a, b, idesc, ks ? 1u : keep);
+                        mma_bf16(dacc, a, b + b_lo_off, idesc, 1u);
+                        mma_bf16(dacc, a + a_lo_off, b, idesc, 1u);
                     }
-                    mma_commit(&empty[s]);
                 }
-                mma_commit(crev_free);
+                mma_commit(&empty[s]);
             }
-            __syncwarp();
+            mma_commit(crev_free);
         }
-        // all threads agree on the stream position for the next pass
-        it = (jc + 1) * W;
+        __syncwarp();
     }
     if (warp == 0 && lane == 0) mma_commit(done);
     __syncwarp();
@@ -462,7 +474,9 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
     if (warp < 4) {
         const bool ok = mbar_wait(done, 0u, err) && !*err;
         tc_fence_after();
-        const int v = warp * 32 + lane;
+        // M = 128: accumulator row v sits in lane v; M = 64: rows 16q .. 16q+15 sit in lanes
+        // 32q .. 32q+15 of lane quarter q
+        const int v = g.M == 128 ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : g.M);
         for (int u0 = 0; u0 < g.N; u0 += 16) {
             float d[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)u0, d);
