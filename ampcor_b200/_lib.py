@@ -102,6 +102,8 @@ SIGNATURES = {
                                    POINTER(ctypes.c_double), POINTER(c_uint64)]),
     "ampcor_kernel_times": (c_int, [c_void_p, POINTER(ctypes.c_double), POINTER(c_uint64)]),
     "ampcor_form": (c_int, [c_void_p]),
+    "ampcor_configure": (c_int, [c_void_p, c_int, c_uint64]),
+    "ampcor_chunk": (c_int, [c_void_p, POINTER(c_uint64)]),
     "ampcor_correlate_noalloc": (c_int, [POINTER(Params), POINTER(Job), c_void_p, ctypes.c_char_p,
                                          ctypes.c_size_t]),
     "ampcor_last_error": (c_char_p, [c_void_p]),

@@ -260,6 +260,7 @@ struct ampcor_handle {
     float* d_chip_taps = nullptr;
     float* d_win_taps = nullptr;
     float* d_zoom_taps = nullptr;
+    float* d_zoom_ut = nullptr;
     // arena API
     float2* h_arena = nullptr;
     float2* d_arena = nullptr;
@@ -276,6 +277,7 @@ struct ampcor_handle {
     // refined amplitudes of one chunk of pairs
     float* d_refined = nullptr;
     size_t chunk = 0;
+    size_t chunk_override = 0;
     long long refined_stride = 0;
     // host-path staging
     void* d_ref_raster = nullptr;
@@ -384,7 +386,7 @@ size_t default_chunk()
 int ensure_refined(ampcor_handle* h)
 {
     if (h->d_refined) return AMPCOR_OK;
-    h->chunk = default_chunk();
+    h->chunk = h->chunk_override ? h->chunk_override : default_chunk();
     h->refined_stride = (long long)h->Rf * h->Rf + (long long)h->Wf * h->Wf;
     cudaError_t e = cudaMalloc(&h->d_refined, h->chunk * h->refined_stride * sizeof(float));
     if (e != cudaSuccess) {
@@ -508,8 +510,8 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
                                                           h->d_tc_err);
         cudaEvent_t f = mark(h, st);
         keep(h, 2, e, f);
-        zoom_kernel<<<n, kThreads, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg,
-                                                       h->d_zoom_taps, h->d_coarse, h->d_coarse_peak,
+        zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg,
+                                                  h->d_zoom_ut, h->d_coarse, h->d_coarse_peak,
                                                        h->d_fine_out, h->M, h->f, h->m, compat,
                                                        offsets, diag);
         keep(h, 5, f, mark(h, st));
@@ -601,7 +603,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         h->tensor = want && plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
         h->gsc = stats_layout(h->gc);
         h->gsf = stats_layout(h->gf);
-        h->zoom_smem = (round4(h->Cf * h->Cf) + round4(h->Cf * h->Z) + round4(h->z * h->zg.taps_len) + 64) * 4;
+        const int Zp = (h->Z + 7) & ~7;
+        h->zoom_smem = (round4(h->Cf * h->Cf) + 2 * h->Cf * Zp + 64) * 4;
     }
 
     cudaError_t e = cudaSetDevice(p->device);
@@ -639,6 +642,18 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     const std::vector<float> ct = taps_table(h->R, h->f, 1, h->ic.taps_len);
     const std::vector<float> wt = taps_table(h->E, h->f, 1, h->iw.taps_len);
     const std::vector<float> zt = taps_table(h->Cf, h->z, 0, h->zg.taps_len);
+    // transposed zoom interpolation matrix, Ut[l][q] = D_Cf(q / z - l), rows padded to 8
+    std::vector<float> zut;
+    {
+        const int Zp = (h->Z + 7) & ~7;
+        zut.assign((size_t)h->Cf * Zp, 0.0f);
+        for (int l = 0; l < h->Cf; ++l)
+            for (int q = 0; q < h->Z; ++q) {
+                const int s = q % h->z, b = q / h->z;
+                zut[(size_t)l * Zp + q] = s == 0 ? (b == l ? 1.0f : 0.0f)
+                                                 : (float)dirichlet(h->Cf, (double)q / h->z - l);
+            }
+    }
     auto upload = [&](float*& d, const std::vector<float>& v) {
         cudaError_t ue = cudaMalloc(&d, std::max<size_t>(v.size(), 1) * sizeof(float));
         if (ue != cudaSuccess) return ue;
@@ -646,7 +661,7 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         return ue;
     };
     if ((e = upload(h->d_chip_taps, ct)) != cudaSuccess || (e = upload(h->d_win_taps, wt)) != cudaSuccess ||
-        (e = upload(h->d_zoom_taps, zt)) != cudaSuccess)
+        (e = upload(h->d_zoom_taps, zt)) != cudaSuccess || (e = upload(h->d_zoom_ut, zut)) != cudaSuccess)
         return cuda_create_fail(e, "uploading interpolation taps");
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess ||
@@ -665,6 +680,7 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_chip_taps);
     cudaFree(h->d_win_taps);
     cudaFree(h->d_zoom_taps);
+    cudaFree(h->d_zoom_ut);
     cudaFree(h->d_arena);
     cudaFree(h->d_ref_off);
     cudaFree(h->d_tgt_off);
@@ -919,6 +935,49 @@ int ampcor_kernel_times(ampcor_handle* h, double* ms, uint64_t* launches)
         }
     }
     drop_marks(h);
+    return AMPCOR_OK;
+}
+
+int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
+{
+    if (!h) return AMPCOR_E_ARG;
+    CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
+    CK(h, cudaStreamSynchronize(h->stream), "waiting for the worker");
+    if (form == 1) {
+        std::string terr;
+        if (!plan_tc(h->R, h->W, 8, h->tcc, terr) || !plan_tc(h->Rf, h->Wf, 4, h->tcf, terr))
+            return fail(h, AMPCOR_E_SHAPE, "this geometry has no tensor-core form: " + terr);
+        h->tensor = true;
+    } else if (form == 0) {
+        h->tensor = false;
+    } else if (form != -1) {
+        return fail(h, AMPCOR_E_ARG, "form must be -1, 0 or 1");
+    }
+    if (chunk && chunk != h->chunk) {
+        // the chunk scratch is sized on first use
+        cudaFree(h->d_refined);
+        cudaFree(h->d_inv_c);
+        cudaFree(h->d_inv_f);
+        cudaFree(h->d_gam);
+        h->d_refined = nullptr;
+        h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
+        h->chunk_override = (size_t)chunk;
+    } else if (form != -1 && h->d_refined) {
+        // a form switch needs the tensor-form scratch of the current chunk
+        cudaFree(h->d_refined);
+        cudaFree(h->d_inv_c);
+        cudaFree(h->d_inv_f);
+        cudaFree(h->d_gam);
+        h->d_refined = nullptr;
+        h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
+    }
+    return AMPCOR_OK;
+}
+
+int ampcor_chunk(const ampcor_handle* h, uint64_t* chunk)
+{
+    if (!h || !chunk) return AMPCOR_E_ARG;
+    *chunk = h->chunk_override ? h->chunk_override : default_chunk();
     return AMPCOR_OK;
 }
 

@@ -90,6 +90,27 @@ __device__ void block_argmax(float& bv, int& bi, float* redf, int* redi)
     __syncthreads();
 }
 
+template <int NT>
+__device__ void block_argmax_n(float& bv, int& bi, float* redf, int* redi)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        better(bv, bi, ov, oi);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        redf[warp] = bv;
+        redi[warp] = bi;
+    }
+    __syncthreads();
+    bv = redf[0];
+    bi = redi[0];
+    for (int w = 1; w < NT / 32; ++w) better(bv, bi, redf[w], redi[w]);
+    __syncthreads();
+}
+
 // ------------------------------------------------------------------------------------------
 // correlation numerator: register sliding window along one chip row
 // ------------------------------------------------------------------------------------------
@@ -731,9 +752,16 @@ window_stats_real_kernel(RealTiles t, long long pairs, NccGeom g, float* inv)
                  reinterpret_cast<double*>(smem + g.off_chip));
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+// zoom of the refined surfaces for the tensor-core form: Zm = U G U^T (U = the Z x Cf
+// band-limited interpolation matrix) as two register-tiled products on the FP32 pipes, each
+// thread owning an 8 x 8 block of outputs (64 FMAs per four 128-bit shared loads), the zoomed
+// surface reduced straight to its first maximum.  Zp = Z rounded up to 8; padded rows/columns
+// of U are zero and never win the maximum.
+constexpr int kZoomThreads = 256;
+
+__global__ void __launch_bounds__(kZoomThreads, 2)
 zoom_kernel(const float* gam, long long pair0, long long pairs, const long long* ref_off,
-            ZoomGeom zg, const float* zoom_taps, const CoarseOut* coarse, const float* coarse_peak,
+            ZoomGeom zg, const float* zoom_ut, const CoarseOut* coarse, const float* coarse_peak,
             const FineOut* fout, int margin, int refine_factor, int refine_margin, int ref_compat,
             float2* offsets, PairDiag* diag)
 {
@@ -747,23 +775,68 @@ zoom_kernel(const float* gam, long long pair0, long long pairs, const long long*
         }
         return;
     }
-    const int Cf = zg.Cf;
-    float* G = smem;
-    float* T = G + ((Cf * Cf + 3) & ~3);
-    float* taps = T + ((Cf * zg.Z + 3) & ~3);
-    float* red = taps + ((zg.z * zg.taps_len + 3) & ~3);
+    const int Cf = zg.Cf, Z = zg.Z, Zp = (Z + 7) & ~7, nt = Zp / 8;
+    float* G = smem;                          // Cf x Cf
+    float* Ut = G + ((Cf * Cf + 3) & ~3);     // Cf x Zp: Ut[l][q] = U[q][l]
+    float* T = Ut + Cf * Zp;                  // Cf x Zp: T[a][q] = sum_l G[a][l] U[q][l]
+    float* red = T + Cf * Zp;
     const float* src = gam + (long long)blockIdx.x * Cf * Cf;
-    for (int idx = threadIdx.x; idx < Cf * Cf; idx += kThreads) G[idx] = src[idx];
-    for (int idx = threadIdx.x; idx < zg.z * zg.taps_len; idx += kThreads) taps[idx] = __ldg(zoom_taps + idx);
+    for (int idx = threadIdx.x; idx < Cf * Cf; idx += kZoomThreads) G[idx] = src[idx];
+    for (int idx = threadIdx.x; idx < Cf * Zp / 4; idx += kZoomThreads)
+        reinterpret_cast<float4*>(Ut)[idx] = __ldg(reinterpret_cast<const float4*>(zoom_ut) + idx);
     __syncthreads();
-    float zv;
-    int zi;
-    zoom_argmax(G, T, taps, zg, zv, zi);
-    block_argmax(zv, zi, red, reinterpret_cast<int*>(red + kWarps));
+    // T: Cf x (Zp/8) strips of 8 outputs
+    for (int t = threadIdx.x; t < Cf * nt; t += kZoomThreads) {
+        const int a = t / nt, q0 = (t - a * nt) * 8;
+        float acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.0f;
+        for (int l = 0; l < Cf; ++l) {
+            const float gv = G[a * Cf + l];
+            const float4 u0 = *reinterpret_cast<const float4*>(Ut + l * Zp + q0);
+            const float4 u1 = *reinterpret_cast<const float4*>(Ut + l * Zp + q0 + 4);
+            acc[0] = fmaf(gv, u0.x, acc[0]); acc[1] = fmaf(gv, u0.y, acc[1]);
+            acc[2] = fmaf(gv, u0.z, acc[2]); acc[3] = fmaf(gv, u0.w, acc[3]);
+            acc[4] = fmaf(gv, u1.x, acc[4]); acc[5] = fmaf(gv, u1.y, acc[5]);
+            acc[6] = fmaf(gv, u1.z, acc[6]); acc[7] = fmaf(gv, u1.w, acc[7]);
+        }
+        *reinterpret_cast<float4*>(T + a * Zp + q0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        *reinterpret_cast<float4*>(T + a * Zp + q0 + 4) = make_float4(acc[4], acc[5], acc[6], acc[7]);
+    }
+    __syncthreads();
+    // Zm: (Zp/8)^2 blocks of 8 x 8
+    float bv = -INFINITY;
+    int bi = INT_MAX;
+    for (int t = threadIdx.x; t < nt * nt; t += kZoomThreads) {
+        const int p0 = (t / nt) * 8, q0 = (t % nt) * 8;
+        float acc[8][8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[i][k] = 0.0f;
+        for (int a = 0; a < Cf; ++a) {
+            const float4 ua = *reinterpret_cast<const float4*>(Ut + a * Zp + p0);
+            const float4 ub = *reinterpret_cast<const float4*>(Ut + a * Zp + p0 + 4);
+            const float4 ta = *reinterpret_cast<const float4*>(T + a * Zp + q0);
+            const float4 tb = *reinterpret_cast<const float4*>(T + a * Zp + q0 + 4);
+            const float uu[8] = {ua.x, ua.y, ua.z, ua.w, ub.x, ub.y, ub.z, ub.w};
+            const float tt[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[i][k] = fmaf(uu[i], tt[k], acc[i][k]);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (p0 + i < Z && q0 + k < Z) better(bv, bi, acc[i][k], (p0 + i) * Z + q0 + k);
+    }
+    block_argmax_n<kZoomThreads>(bv, bi, red, reinterpret_cast<int*>(red + kZoomThreads / 32));
     if (threadIdx.x == 0) {
         const CoarseOut co = coarse[p];
         const FineOut fo = fout[p];
-        const int fp = zi / zg.Z, fq = zi - fp * zg.Z;
+        const int fp = bi / Z, fq = bi - fp * Z;
         const float zoom = (float)(refine_factor * zg.z);
         float dy, dx;
         if (ref_compat) {
@@ -776,7 +849,7 @@ zoom_kernel(const float* gam, long long pair0, long long pairs, const long long*
         offsets[p] = make_float2(dy, dx);
         if (diag) {
             diag[p] = PairDiag{co.u, co.v, co.top, co.left, fo.u, fo.v, fp, fq, coarse_peak[p],
-                               fo.peak, zv, 0.0f};
+                               fo.peak, bv, 0.0f};
         }
     }
 }

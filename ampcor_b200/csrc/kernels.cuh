@@ -169,7 +169,7 @@ __global__ void tc_fine_kernel(RealTiles t, long long pair0, long long pairs, Tc
 
 // zoom of the refined surfaces of a chunk (C^2 floats per chunk-local pair), offsets
 __global__ void zoom_kernel(const float* gam, long long pair0, long long pairs,
-                            const long long* ref_off, ZoomGeom zg, const float* zoom_taps,
+                            const long long* ref_off, ZoomGeom zg, const float* zoom_ut,
                             const CoarseOut* coarse, const float* coarse_peak, const FineOut* fout,
                             int margin, int refine_factor, int refine_margin, int ref_compat,
                             float2* offsets, PairDiag* diag);

@@ -129,6 +129,19 @@ class Worker:
                self._lib.ampcor_stage_times(self._handle, byref(c), byref(r), byref(f), byref(n)))
         return c.value, r.value, f.value, n.value
 
+    def configure(self, form=None, chunk=None):
+        """Select the form ("tensor" or "plain") and the refinement chunk (pairs)."""
+        f = {None: -1, "plain": 0, "tensor": 1}[form]
+        _check(self._lib, self._handle,
+               self._lib.ampcor_configure(self._handle, f, int(chunk or 0)))
+        self.form = "tensor" if self._lib.ampcor_form(self._handle) == 1 else "plain"
+
+    @property
+    def chunk(self):
+        c = ctypes.c_uint64()
+        _check(self._lib, self._handle, self._lib.ampcor_chunk(self._handle, byref(c)))
+        return c.value
+
     KERNELS = ("coarse_correlation", "refinement", "fine_correlation", "coarse_statistics",
                "fine_statistics", "zoom")
 

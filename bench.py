@@ -46,10 +46,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--plain", action="store_true",
-                    help="plain FP32 form instead of the tensor-core form")
+                    help="plain FP32 form only (no tensor-core candidates)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (default form and chunk)")
     ap.add_argument("--pairs", type=int, default=0,
                     help="correlate only the first N pairs (small cases for profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-jobs", type=int, default=40)
     return ap.parse_args()
 
 
@@ -229,6 +233,13 @@ def run_b200(args):
     ulhc = torch.from_numpy(w.ulhc).to(dev)
     offsets = torch.empty((w.pairs, 2), dtype=torch.float32, device=dev)
 
+    tuned = None
+    if not args.no_tune:
+        from ampcor_b200.autotune import tune
+
+        forms = ("plain",) if args.plain else ("tensor", "plain")
+        tuned = tune(worker, ref, tgt, ulhc, forms=forms, use_cache=False)
+
     def step():
         worker.correlate(ref, tgt, ulhc, offsets=offsets, synchronize=False)
 
@@ -344,7 +355,11 @@ def run_b200(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16x3" if worker.form == "tensor" else "f32",
-            "data": "synthetic", "config": dict(workload_config(w), form=worker.form),
+            "data": "synthetic",
+            "config": dict(workload_config(w), form=worker.form, chunk=worker.chunk,
+                           autotuned=tuned is not None,
+                           tune=[(c["form"], c["chunk"], round(c["ms"], 3)) for c in tuned["candidates"]]
+                           if tuned else None),
             "roofline": {
                 "bound": "tensor", "kernel": names[top], "achieved": achieved,
                 "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved / tensor_peak,
@@ -365,11 +380,30 @@ def run_b200(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_serving:
+            line["serving"] = serving_run(local, args)
         print(json.dumps(line), flush=True)
     worker.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def serving_run(device, args):
+    """p50 / p99 job latency of the continuous-batching loop under a seeded Poisson stream."""
+    from ampcor_b200 import serve
+
+    jobs = serve.poisson_jobs(args.serving_jobs, rate=20.0, seed=7, device=f"cuda:{device}",
+                              sizes=(1024, 2048, 4096), chips=(32, 64), margins=(16, 32),
+                              zooms=(8, 16), spacing=(64, 128), pinned=False)
+    srv = serve.Server(device=device, slots=4)
+    srv.warm(jobs)
+    srv.run(jobs, realtime=True)
+    rep = serve.latency_report(jobs)
+    rep["stream"] = (f"{args.serving_jobs} jobs, Poisson 20 jobs/s (seed 7), rasters 1024-4096 "
+                     f"px per side resident in HBM, chip 32/64, margin 16/32, refine 2, zoom 8/16, "
+                     f"4 slots")
+    return rep
 
 
 def worker_chunk():

@@ -181,6 +181,14 @@ int ampcor_kernel_times(ampcor_handle* handle, double* ms, uint64_t* launches);
    reference counterpart. */
 int ampcor_form(const ampcor_handle* handle);
 
+/* Choose the correlation form (form: 1 tensor cores, 0 plain FP32, -1 unchanged) and the number
+   of pairs refined per chunk (chunk: 0 unchanged), as an autotuner does.  Waits for the worker's
+   stream.  No reference counterpart. */
+int ampcor_configure(ampcor_handle* handle, int form, uint64_t chunk);
+
+/* The number of pairs refined per chunk. */
+int ampcor_chunk(const ampcor_handle* handle, uint64_t* chunk);
+
 /* Message of the last failure on handle (or of the last failed ampcor_create when handle is
    NULL). */
 const char* ampcor_last_error(const ampcor_handle* handle);
