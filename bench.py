@@ -53,6 +53,7 @@ def parse():
                     help="correlate only the first N pairs (small cases for profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--serving-jobs", type=int, default=40)
     return ap.parse_args()
 
@@ -382,6 +383,8 @@ def run_b200(args):
             line["cpu_baseline"] = cpu
         if world == 1 and not args.no_serving:
             line["serving"] = serving_run(local, args)
+        if world == 1 and not args.no_uneven:
+            line["batched_uneven"] = uneven_run(local, args)
         print(json.dumps(line), flush=True)
     worker.close()
     if world > 1:
@@ -404,6 +407,41 @@ def serving_run(device, args):
                      f"px per side resident in HBM, chip 32/64, margin 16/32, refine 2, zoom 8/16, "
                      f"4 slots")
     return rep
+
+
+def uneven_run(device, args):
+    """Throughput of the batched uneven configuration: 16 raster pairs of different sizes and
+    geometries, every geometry autotuned, all work replayed as one CUDA graph."""
+    import torch
+
+    from ampcor_b200 import batch
+
+    jobs = batch.uneven_jobs(16, seed=11, device=f"cuda:{device}")
+    ub = batch.UnevenBatch(jobs, device=device, tune=True)
+    ub.capture()
+    for _ in range(2):
+        ub.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(ub.stream)
+    for _ in range(reps):
+        ub.replay()
+    e1.record(ub.stream)
+    torch.cuda.synchronize()
+    ub.check()
+    ms = e0.elapsed_time(e1) / reps
+    geoms = sorted({j.geometry for j in jobs})
+    out = {
+        "raster_pairs": len(jobs), "pairs": ub.pairs, "ms_per_batch": ms,
+        "pairs_per_s": ub.pairs / (ms / 1e3),
+        "geometries": [f"chip {g[0]} margin {g[1]} zoom {g[4]}: "
+                       f"{ub.tuning[g]['form']} chunk {ub.tuning[g]['chunk']}" for g in geoms],
+        "launch": "one CUDA graph replay per batch",
+    }
+    ub.close()
+    return out
 
 
 def worker_chunk():
