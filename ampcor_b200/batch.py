@@ -144,7 +144,11 @@ class UnevenBatch:
         return self.graph
 
     def replay(self):
-        self.graph.replay()
+        """Launch the whole batch (one graph launch) on the batch's stream."""
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            self.graph.replay()
 
     def check(self):
         for w in self.workers.values():

@@ -425,10 +425,11 @@ def uneven_run(device, args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     reps = 5
-    e0.record(ub.stream)
-    for _ in range(reps):
-        ub.replay()
-    e1.record(ub.stream)
+    with torch.cuda.stream(ub.stream):
+        e0.record()
+        for _ in range(reps):
+            ub.replay()
+        e1.record()
     torch.cuda.synchronize()
     ub.check()
     ms = e0.elapsed_time(e1) / reps
