@@ -44,7 +44,7 @@ def _store(table):
         pass
 
 
-def tune(worker, ref, tgt, ulhc, forms=("tensor", "plain"), chunks=DEFAULT_CHUNKS, reps=2,
+def tune(worker, ref, tgt, ulhc, forms=("spectral", "tensor", "plain"), chunks=DEFAULT_CHUNKS, reps=2,
          use_cache=True):
     """Configure ``worker`` with the fastest (form, chunk) for this batch; returns the choice
     with the timings of every candidate (ms per batch)."""

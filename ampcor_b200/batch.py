@@ -118,7 +118,7 @@ class UnevenBatch:
             if tune:
                 from .autotune import tune as run_tune
 
-                forms = ("plain",) if plain else ("tensor", "plain")
+                forms = ("plain",) if plain else ("spectral", "tensor", "plain")
                 self.tuning[j.geometry] = run_tune(w, j.ref, j.tgt, u, forms=forms,
                                                    chunks=(296, 592, 1184), reps=1,
                                                    use_cache=False)

@@ -34,6 +34,11 @@ std::string g_create_error;
 
 constexpr int kCompiledNV[] = {9, 16, 17, 32, 33};
 
+// correlation forms (the values ampcor_form returns and ampcor_configure takes)
+constexpr int kFormPlain = 0;
+constexpr int kFormTensor = 1;
+constexpr int kFormSpectral = 2;
+
 int round_nv(int w)
 {
     for (int nv : kCompiledNV)
@@ -208,6 +213,68 @@ bool plan_tc(int R, int W, int raw_bytes, TcGeom& g, std::string& err)
     return true;
 }
 
+// the spectral form of one surface: transform length N >= W from the compiled lengths; shared
+// memory: the N x (N + 1) complex tile, twiddles, the partner table of the spectrum product and
+// a reduction scratch
+bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
+{
+    std::memset(&g, 0, sizeof(g));
+    g.R = R;
+    g.W = W;
+    g.C = W - R + 1;
+    g.N = spec_next_length(W);
+    if (g.N == 0 || !spec_radices(g.N, g.N1, g.N2)) {
+        err = "the spectral form needs a window of at most 160 samples";
+        return false;
+    }
+    auto up = [](long x, long a) { return (x + a - 1) / a * a; };
+    g.RS = g.N + 1;
+    long off = up((long)g.N * g.RS * 8, 16);
+    g.off_z = 0;
+    g.off_tw = (int)off;
+    off = up(off + (long)g.N * 8, 16);
+    g.off_neg = (int)off;
+    off = up(off + (long)g.N * 4, 16);
+    g.off_red = (int)off;
+    off += 256;
+    if (off > 227L * 1024) {
+        err = "tile geometry too large for the spectral form";
+        return false;
+    }
+    g.smem_bytes = (int)off;
+    return true;
+}
+
+// placement statistics kernel: column-sum slices sized so that two CTAs fit on an SM
+bool plan_box(int R, int W, BoxGeom& g, std::string& err)
+{
+    std::memset(&g, 0, sizeof(g));
+    g.R = R;
+    g.W = W;
+    g.C = W - R + 1;
+    g.VS = W + 1;
+    g.nb = std::max(1, kThreads / W);
+    const long row_bytes = 2L * g.VS * 8;
+    g.SU = (int)std::min<long>(g.C, (113L * 1024) / row_bytes);
+    if (g.SU < 1) {
+        err = "window too wide for the placement statistics kernel";
+        return false;
+    }
+    g.smem_bytes = (int)(g.SU * row_bytes);
+    return true;
+}
+
+// exp(-2 pi i m / N), m < N, rounded from FP64
+std::vector<float> spec_twiddle_table(int N)
+{
+    std::vector<float> t(2 * (size_t)N);
+    for (int m = 0; m < N; ++m) {
+        t[2 * m] = (float)std::cos(2.0 * M_PI * m / N);
+        t[2 * m + 1] = (float)-std::sin(2.0 * M_PI * m / N);
+    }
+    return t;
+}
+
 // shared memory of the statistics kernels: the staged window and the FP64 column-sum chunk
 // (unpadded window rows: the statistics walk columns, one thread per column; the chunk of
 // column sums shrinks until two CTAs fit on an SM)
@@ -289,8 +356,16 @@ struct ampcor_handle {
     size_t job_offsets_cap = 0;
     ampcor_pair_diag* d_job_diag = nullptr;
     size_t job_diag_cap = 0;
+    // correlation form (kFormPlain, kFormTensor, kFormSpectral)
+    int form = 0;
+    SpecGeom spc{}, spf{};
+    BoxGeom bxc{}, bxf{};
+    float* d_tw_c = nullptr;
+    float* d_tw_f = nullptr;
+    // amplitude rasters of the spectral form (reference and secondary, one allocation)
+    float* d_amp = nullptr;
+    size_t amp_cap = 0;
     // tensor-core form
-    bool tensor = false;
     TcGeom tcc{}, tcf{};
     NccGeom gsc{}, gsf{};
     int zoom_smem = 0;
@@ -393,13 +468,13 @@ int ensure_refined(ampcor_handle* h)
         h->d_refined = nullptr;
         return fail(h, AMPCOR_E_NOMEM, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
     }
-    if (h->tensor) {
-        const size_t n = h->chunk;
-        if (cudaMalloc(&h->d_inv_c, n * h->C * h->C * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&h->d_inv_f, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&h->d_gam, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess)
-            return fail(h, AMPCOR_E_NOMEM, "allocating tensor-core form scratch");
-    }
+    const size_t n = h->chunk;
+    if (h->form != kFormPlain &&
+        (cudaMalloc(&h->d_inv_c, n * h->C * h->C * sizeof(float)) != cudaSuccess ||
+         cudaMalloc(&h->d_inv_f, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess))
+        return fail(h, AMPCOR_E_NOMEM, "allocating placement statistics scratch");
+    if (h->form != kFormPlain && cudaMalloc(&h->d_gam, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess)
+        return fail(h, AMPCOR_E_NOMEM, "allocating refined-surface scratch");
     return AMPCOR_OK;
 }
 
@@ -520,11 +595,82 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
     return AMPCOR_OK;
 }
 
+// spectral form: amplitudes of both rasters once, then per chunk: coarse statistics -> coarse
+// correlation (FFT) -> refinement -> fine statistics -> fine correlation (FFT) -> zoom
+int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+{
+    if (pairs == 0) return AMPCOR_OK;
+    int rc = ensure_refined(h);
+    if (rc) return rc;
+    if ((rc = ensure_fine_out(h, (size_t)pairs))) return rc;
+    const bool shared = src.ref_base == src.tgt_base;
+    const size_t need = (size_t)src.ref_count + (shared ? 0 : (size_t)src.tgt_count);
+    if ((rc = grow(h, h->d_amp, h->amp_cap, need, "amplitude rasters"))) return rc;
+    float* amp_ref = h->d_amp;
+    float* amp_tgt = shared ? h->d_amp : h->d_amp + src.ref_count;
+    auto detect = [&](const float2* x, long long n, float* y) {
+        const long long blocks = std::min<long long>((n + 1023) / 1024, 148 * 16);
+        if (n > 0) detect_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, st>>>(x, n, y);
+    };
+    cudaEvent_t a0 = mark(h, st);
+    detect(src.ref_base, src.ref_count, amp_ref);
+    if (!shared) detect(src.tgt_base, src.tgt_count, amp_tgt);
+    CK(h, cudaGetLastError(), "launching the detection kernel");
+    keep(h, 3, a0, mark(h, st));
+    const SpecSource cs{amp_ref, src.ref_stride, src.ref_off, 0, amp_tgt, src.tgt_stride, src.tgt_off, 0};
+    const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
+                        h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
+    const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
+    for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
+        const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
+        cudaEvent_t a = mark(h, st);
+        box_stats_kernel<<<n, kThreads, h->bxc.smem_bytes, st>>>(cs, c0, n, src.ref_off, h->bxc, h->d_inv_c);
+        CK(h, cudaGetLastError(), "launching the coarse statistics kernel");
+        cudaEvent_t b = mark(h, st);
+        keep(h, 3, a, b);
+        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, h->d_inv_c,
+                          reinterpret_cast<const float2*>(h->d_tw_c),
+                          SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
+           "launching the spectral coarse correlation");
+        cudaEvent_t c = mark(h, st);
+        keep(h, 0, b, c);
+        refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
+                                                           h->d_chip_taps, h->d_win_taps,
+                                                           h->d_refined, h->refined_stride);
+        CK(h, cudaGetLastError(), "launching the refinement kernel");
+        cudaEvent_t d = mark(h, st);
+        keep(h, 1, c, d);
+        box_stats_kernel<<<n, kThreads, h->bxf.smem_bytes, st>>>(fs, c0, n, src.ref_off, h->bxf, h->d_inv_f);
+        CK(h, cudaGetLastError(), "launching the fine statistics kernel");
+        cudaEvent_t e = mark(h, st);
+        keep(h, 4, d, e);
+        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, h->d_inv_f,
+                          reinterpret_cast<const float2*>(h->d_tw_f),
+                          SpecOut{1, 0, nullptr, nullptr, h->d_fine_out, h->d_gam, refined_surfaces}),
+           "launching the spectral fine correlation");
+        cudaEvent_t f = mark(h, st);
+        keep(h, 2, e, f);
+        zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg, h->d_zoom_ut,
+                                                  h->d_coarse, h->d_coarse_peak, h->d_fine_out, h->M,
+                                                  h->f, h->m, compat, offsets, diag);
+        CK(h, cudaGetLastError(), "launching the zoom kernel");
+        keep(h, 5, f, mark(h, st));
+    }
+    return AMPCOR_OK;
+}
+
 int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
                  PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
 {
-    return h->tensor ? run_tensor(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st)
-                     : run_plain(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+    switch (h->form) {
+        case kFormSpectral:
+            return run_spectral(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+        case kFormTensor:
+            return run_tensor(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+        default:
+            return run_plain(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+    }
 }
 
 cudaStream_t pick(ampcor_handle* h, void* stream)
@@ -593,14 +739,19 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         return create_fail(AMPCOR_E_SHAPE, err);
     }
     h->refine_smem = std::max(h->ic.smem_bytes, h->iw.smem_bytes);
-    // the tensor-core form unless the plain FP32 form is asked for or the geometry needs it
+    // the spectral form where the geometry allows it, else the tensor-core form, else the plain
+    // form; AMPCOR_FLAG_PLAIN_FP32 (or AMPCOR_FORM=plain|tensor|spectral) chooses
     {
-        const char* form = std::getenv("AMPCOR_FORM");
-        bool want = !(p->flags & AMPCOR_FLAG_PLAIN_FP32);
-        if (form && std::strcmp(form, "plain") == 0) want = false;
-        if (form && std::strcmp(form, "tensor") == 0) want = true;
+        const char* env = std::getenv("AMPCOR_FORM");
         std::string terr;
-        h->tensor = want && plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
+        const bool spec_ok = plan_spec(h->R, h->W, h->spc, terr) && plan_spec(h->Rf, h->Wf, h->spf, terr) &&
+                             plan_box(h->R, h->W, h->bxc, terr) && plan_box(h->Rf, h->Wf, h->bxf, terr);
+        const bool tc_ok = plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
+        h->form = spec_ok ? kFormSpectral : tc_ok ? kFormTensor : kFormPlain;
+        if (p->flags & AMPCOR_FLAG_PLAIN_FP32) h->form = kFormPlain;
+        if (env && std::strcmp(env, "plain") == 0) h->form = kFormPlain;
+        if (env && std::strcmp(env, "tensor") == 0 && tc_ok) h->form = kFormTensor;
+        if (env && std::strcmp(env, "spectral") == 0 && spec_ok) h->form = kFormSpectral;
         h->gsc = stats_layout(h->gc);
         h->gsf = stats_layout(h->gf);
         const int Zp = (h->Z + 7) & ~7;
@@ -636,7 +787,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         (e = cudaFuncSetAttribute(tc_fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(zoom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kMaxSmem)) != cudaSuccess)
+                                  kMaxSmem)) != cudaSuccess ||
+        (e = spec_set_smem_limits()) != cudaSuccess)
         return cuda_create_fail(e, "configuring kernel shared memory");
 
     const std::vector<float> ct = taps_table(h->R, h->f, 1, h->ic.taps_len);
@@ -661,7 +813,9 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         return ue;
     };
     if ((e = upload(h->d_chip_taps, ct)) != cudaSuccess || (e = upload(h->d_win_taps, wt)) != cudaSuccess ||
-        (e = upload(h->d_zoom_taps, zt)) != cudaSuccess || (e = upload(h->d_zoom_ut, zut)) != cudaSuccess)
+        (e = upload(h->d_zoom_taps, zt)) != cudaSuccess || (e = upload(h->d_zoom_ut, zut)) != cudaSuccess ||
+        (e = upload(h->d_tw_c, spec_twiddle_table(std::max(h->spc.N, 1)))) != cudaSuccess ||
+        (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->spf.N, 1)))) != cudaSuccess)
         return cuda_create_fail(e, "uploading interpolation taps");
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess ||
@@ -699,6 +853,9 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_inv_f);
     cudaFree(h->d_gam);
     cudaFree(h->d_fine_out);
+    cudaFree(h->d_tw_c);
+    cudaFree(h->d_tw_f);
+    cudaFree(h->d_amp);
     cudaFree(h->d_tc_err);
     drop_marks(h);
     if (h->h_arena) cudaFreeHost(h->h_arena);
@@ -766,7 +923,8 @@ int ampcor_adjust(ampcor_handle* h, const float** offsets)
         arena_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
             (long long)P, (long long)h->R * h->R, (long long)h->W * h->W, h->d_ref_off, h->d_tgt_off);
         CK(h, cudaGetLastError(), "launching the arena offsets kernel");
-        PairSource src{h->d_arena, h->d_ref_off, h->R, h->d_arena, h->d_tgt_off, h->W};
+        const long long cells = (long long)P * ((long long)h->R * h->R + (long long)h->W * h->W);
+        PairSource src{h->d_arena, h->d_ref_off, h->R, h->d_arena, h->d_tgt_off, h->W, cells, cells};
         if ((rc = run_pipeline(h, src, (long long)P, h->d_offsets, h->d_diag, nullptr, nullptr, st))) return rc;
         CK(h, cudaMemcpyAsync(h->h_offsets, h->d_offsets, 2 * P * sizeof(float), cudaMemcpyDeviceToHost, st),
            "harvesting the offset field");
@@ -812,7 +970,8 @@ int ampcor_correlate(ampcor_handle* h, const ampcor_job* j, void* stream)
         h->R, h->W, h->d_ref_off, h->d_tgt_off, h->d_bad);
     CK(h, cudaGetLastError(), "launching the pair offsets kernel");
     PairSource src{static_cast<const float2*>(j->ref), h->d_ref_off, j->ref_samples,
-                   static_cast<const float2*>(j->tgt), h->d_tgt_off, j->tgt_samples};
+                   static_cast<const float2*>(j->tgt), h->d_tgt_off, j->tgt_samples,
+                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples};
     return run_pipeline(h, src, (long long)j->pairs, reinterpret_cast<float2*>(j->offsets),
                         reinterpret_cast<PairDiag*>(j->diag), j->coarse_surfaces,
                         j->refined_surfaces, st);
@@ -943,16 +1102,20 @@ int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
     if (!h) return AMPCOR_E_ARG;
     CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
     CK(h, cudaStreamSynchronize(h->stream), "waiting for the worker");
-    if (form == 1) {
+    if (form == kFormTensor) {
         std::string terr;
         if (!plan_tc(h->R, h->W, 8, h->tcc, terr) || !plan_tc(h->Rf, h->Wf, 4, h->tcf, terr))
             return fail(h, AMPCOR_E_SHAPE, "this geometry has no tensor-core form: " + terr);
-        h->tensor = true;
-    } else if (form == 0) {
-        h->tensor = false;
-    } else if (form != -1) {
-        return fail(h, AMPCOR_E_ARG, "form must be -1, 0 or 1");
+    } else if (form == kFormSpectral) {
+        std::string terr;
+        if (!plan_spec(h->R, h->W, h->spc, terr) || !plan_spec(h->Rf, h->Wf, h->spf, terr) ||
+            !plan_box(h->R, h->W, h->bxc, terr) || !plan_box(h->Rf, h->Wf, h->bxf, terr))
+            return fail(h, AMPCOR_E_SHAPE, "this geometry has no spectral form: " + terr);
+    } else if (form != kFormPlain && form != -1) {
+        return fail(h, AMPCOR_E_ARG, "form must be -1, 0, 1 or 2");
     }
+    const bool switching = form != -1 && form != h->form;
+    if (form != -1) h->form = form;
     if (chunk && chunk != h->chunk) {
         // the chunk scratch is sized on first use
         cudaFree(h->d_refined);
@@ -962,8 +1125,8 @@ int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
         h->d_refined = nullptr;
         h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
         h->chunk_override = (size_t)chunk;
-    } else if (form != -1 && h->d_refined) {
-        // a form switch needs the tensor-form scratch of the current chunk
+    } else if (switching && h->d_refined) {
+        // a form switch needs the chunk scratch of the new form
         cudaFree(h->d_refined);
         cudaFree(h->d_inv_c);
         cudaFree(h->d_inv_f);
@@ -984,7 +1147,7 @@ int ampcor_chunk(const ampcor_handle* h, uint64_t* chunk)
 int ampcor_form(const ampcor_handle* h)
 {
     if (!h) return -1;
-    return h->tensor ? 1 : 0;
+    return h->form;
 }
 
 int ampcor_surface_dims(const ampcor_handle* h, int32_t* coarse, int32_t* refined, int32_t* zoomed)
@@ -1166,7 +1329,8 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
     pair_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
         j->ulhc, P, j->ref_lines, j->ref_samples, j->tgt_lines, j->tgt_samples, R, W, ref_off, tgt_off, bad);
     PairSource src{static_cast<const float2*>(j->ref), ref_off, j->ref_samples,
-                   static_cast<const float2*>(j->tgt), tgt_off, j->tgt_samples};
+                   static_cast<const float2*>(j->tgt), tgt_off, j->tgt_samples,
+                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples};
     coarse_kernel<<<(unsigned)P, kThreads, gc.smem_bytes, st>>>(src, 0, P, gc, m, coarse, peak,
                                                                 j->coarse_surfaces);
     const int refine_smem = std::max(ic.smem_bytes, iw.smem_bytes);

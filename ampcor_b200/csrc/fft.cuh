@@ -1,0 +1,388 @@
+// Shared-memory FFTs of the spectral correlation form (host + device templates).
+//
+// A length-N transform (N = N1 * N2, both at most 16 and built from the radices 2, 3, 4, 5) runs
+// as two in-place steps over a row or column of a 2-D tile:
+//
+//   n = N2 n1 + n2,  k = k1 + N1 k2
+//   step A (one task per n2): y[k1] = DFT_N1(x[N2 n1 + n2])[k1] * W_N^(n2 k1), stored where
+//                             x[N2 k1 + n2] was
+//   step B (one task per k1): X[k1 + N1 k2] = DFT_N2(y[N2 k1 + n2])[k2], stored at N2 k1 + k2
+//
+// so the spectrum sits in a fixed permutation of the frequencies (position N2 k1 + k2 holds
+// frequency k1 + N1 k2) and the inverse runs the two steps backwards from that permutation to
+// natural order.  Neither step needs a scratch buffer: a task reads and writes the same positions.
+// The short DFTs run in registers (mixed-radix Cooley-Tukey over compile-time indices); their
+// twiddles come from a compile-time table of cos / sin (2 pi m / 240), evaluated from Taylor
+// series after an exact reduction of m to the first octant.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#ifndef HD
+#define HD __host__ __device__ __forceinline__
+#endif
+
+namespace ampcor_b200 {
+namespace fft {
+
+// ---- compile-time cos / sin of 2 pi m / 240 -------------------------------------------------
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+constexpr double taylor_cos(double x)
+{
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+
+constexpr double taylor_sin(double x)
+{
+    double term = x, sum = x;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+
+struct Tw240 {
+    float c[240];
+    float s[240];
+};
+
+// angle 2 pi q / 240: quadrant q / 60, remainder r; r <= 30 is within pi/4 of the quadrant start,
+// larger r is within pi/4 of its end
+constexpr Tw240 make_tw240()
+{
+    Tw240 t{};
+    for (int q = 0; q < 240; ++q) {
+        const int quad = q / 60, r = q % 60;
+        double c = 0.0, s = 0.0;
+        if (r <= 30) {
+            const double phi = kPi * r / 120.0;
+            c = taylor_cos(phi);
+            s = taylor_sin(phi);
+        } else {
+            const double phi = kPi * (60 - r) / 120.0;
+            c = taylor_sin(phi);
+            s = taylor_cos(phi);
+        }
+        double cc = c, ss = s;
+        if (quad == 1) {
+            cc = -s;
+            ss = c;
+        } else if (quad == 2) {
+            cc = -c;
+            ss = -s;
+        } else if (quad == 3) {
+            cc = s;
+            ss = -c;
+        }
+        t.c[q] = (float)cc;
+        t.s[q] = (float)ss;
+    }
+    return t;
+}
+
+__constant__ Tw240 kTw240Dev = make_tw240();
+constexpr Tw240 kTw240Host = make_tw240();
+
+HD float tw_cos(int i)
+{
+#ifdef __CUDA_ARCH__
+    return kTw240Dev.c[i];
+#else
+    return kTw240Host.c[i];
+#endif
+}
+
+HD float tw_sin(int i)
+{
+#ifdef __CUDA_ARCH__
+    return kTw240Dev.s[i];
+#else
+    return kTw240Host.s[i];
+#endif
+}
+
+// ---- complex helpers ----------------------------------------------------------------------
+
+HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+HD float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// a * conj(b)
+HD float2 cmulc(float2 a, float2 b) { return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }
+// a * (s i), s = +-1
+template <int S>
+HD float2 mul_si(float2 a) { return S > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); }
+
+// v * exp(S 2 pi i m / N) for a compile-time N (240 % N == 0) and a constant-after-unrolling m
+template <int N, int S>
+HD float2 twiddle(float2 v, int m)
+{
+    static_assert(240 % N == 0, "register DFT length must divide 240");
+    m %= N;
+    if (m == 0) return v;
+    if ((4 * m) % N == 0) {
+        const int j = (4 * m) / N;
+        if (j == 1) return mul_si<S>(v);
+        if (j == 2) return make_float2(-v.x, -v.y);
+        return mul_si<-S>(v);
+    }
+    const int i = m * (240 / N);
+    const float c = tw_cos(i), s = S > 0 ? tw_sin(i) : -tw_sin(i);
+    return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
+// ---- register DFTs (natural order in and out; S = -1 forward, +1 inverse, unnormalised) --------
+
+template <int N, int S>
+struct Dft;
+
+template <int S>
+struct Dft<1, S> {
+    HD static void run(float2 (&)[1]) {}
+};
+
+template <int S>
+struct Dft<2, S> {
+    HD static void run(float2 (&a)[2])
+    {
+        const float2 t = a[0];
+        a[0] = cadd(t, a[1]);
+        a[1] = csub(t, a[1]);
+    }
+};
+
+template <int S>
+struct Dft<3, S> {
+    HD static void run(float2 (&a)[3])
+    {
+        // X1,2 = a0 - (a1 + a2) / 2 +- S i sin(2 pi / 3) (a1 - a2)
+        const float h = 0.866025403784438646763723170752936183f;
+        const float2 t = cadd(a[1], a[2]);
+        const float2 d = csub(a[1], a[2]);
+        const float2 m = make_float2(a[0].x - 0.5f * t.x, a[0].y - 0.5f * t.y);
+        const float2 r = mul_si<S>(make_float2(h * d.x, h * d.y));
+        a[0] = cadd(a[0], t);
+        a[1] = cadd(m, r);
+        a[2] = csub(m, r);
+    }
+};
+
+template <int S>
+struct Dft<4, S> {
+    HD static void run(float2 (&a)[4])
+    {
+        const float2 s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
+        const float2 s13 = cadd(a[1], a[3]), d13 = mul_si<S>(csub(a[1], a[3]));
+        a[0] = cadd(s02, s13);
+        a[2] = csub(s02, s13);
+        a[1] = cadd(d02, d13);
+        a[3] = csub(d02, d13);
+    }
+};
+
+template <int S>
+struct Dft<5, S> {
+    HD static void run(float2 (&a)[5])
+    {
+        // X_k = a0 + sum_{n=1,2} [cos(2 pi n k / 5) (a_n + a_{5-n}) + S i sin(2 pi n k / 5) (a_n - a_{5-n})]
+        const float c1 = 0.309016994374947424102293417182819059f;   // cos(2 pi / 5)
+        const float c2 = -0.809016994374947424102293417182819059f;  // cos(4 pi / 5)
+        const float s1 = 0.951056516295153572116439333379382143f;   // sin(2 pi / 5)
+        const float s2 = 0.587785252292473129168705954639072769f;   // sin(4 pi / 5)
+        const float2 p1 = cadd(a[1], a[4]), m1 = csub(a[1], a[4]);
+        const float2 p2 = cadd(a[2], a[3]), m2 = csub(a[2], a[3]);
+        const float2 a0 = a[0];
+        const float2 r1 = make_float2(a0.x + c1 * p1.x + c2 * p2.x, a0.y + c1 * p1.y + c2 * p2.y);
+        const float2 r2 = make_float2(a0.x + c2 * p1.x + c1 * p2.x, a0.y + c2 * p1.y + c1 * p2.y);
+        // sin(2 pi 2 k / 5) for k = 2 is sin(8 pi / 5) = -sin(2 pi / 5)
+        const float2 i1 = mul_si<S>(make_float2(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y));
+        const float2 i2 = mul_si<S>(make_float2(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y));
+        a[0] = cadd(a0, cadd(p1, p2));
+        a[1] = cadd(r1, i1);
+        a[4] = csub(r1, i1);
+        a[2] = cadd(r2, i2);
+        a[3] = csub(r2, i2);
+    }
+};
+
+// composite N = P Q: n = n1 + P n2, k = Q k1 + k2
+template <int N, int S>
+struct Dft {
+    static constexpr int P = (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : (N % 3 == 0) ? 3 : 5;
+    static constexpr int Q = N / P;
+    static_assert(P * Q == N && Q > 1, "unsupported register DFT length");
+    HD static void run(float2 (&a)[N])
+    {
+        float2 y[P][Q];
+#pragma unroll
+        for (int n1 = 0; n1 < P; ++n1)
+#pragma unroll
+            for (int n2 = 0; n2 < Q; ++n2) y[n1][n2] = a[n1 + P * n2];
+#pragma unroll
+        for (int n1 = 0; n1 < P; ++n1) Dft<Q, S>::run(y[n1]);
+#pragma unroll
+        for (int n1 = 1; n1 < P; ++n1)
+#pragma unroll
+            for (int k2 = 1; k2 < Q; ++k2) y[n1][k2] = twiddle<N, S>(y[n1][k2], n1 * k2);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; ++k2) {
+            float2 t[P];
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) t[n1] = y[n1][k2];
+            Dft<P, S>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) a[Q * k1 + k2] = t[k1];
+        }
+    }
+};
+
+// ---- the two in-place steps of a length N1 N2 transform ----------------------------------
+// base: element 0 of the row or column; es: element stride (1 along a row, the row stride down a
+// column); tw[m] = exp(-2 pi i m / N) for m < N.
+
+template <int N1, int N2>
+HD void fwd_a(float2* base, int es, int n2, const float2* tw)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) a[n1] = base[(N2 * n1 + n2) * es];
+    Dft<N1, -1>::run(a);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[n2 * k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) base[(N2 * k1 + n2) * es] = a[k1];
+}
+
+template <int N1, int N2, int S>
+HD void step_b(float2* base, int es, int k1)
+{
+    float2 a[N2];
+#pragma unroll
+    for (int j = 0; j < N2; ++j) a[j] = base[(N2 * k1 + j) * es];
+    Dft<N2, S>::run(a);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) base[(N2 * k1 + j) * es] = a[j];
+}
+
+template <int N1, int N2>
+HD void inv_a(float2* base, int es, int n2, const float2* tw)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) a[k1] = base[(N2 * k1 + n2) * es];
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmulc(a[k1], tw[n2 * k1]);
+    Dft<N1, 1>::run(a);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) base[(N2 * n1 + n2) * es] = a[n1];
+}
+
+// position of frequency k in the permuted spectrum, and the frequency at position p
+template <int N1, int N2>
+HD int pos_of(int k) { return N2 * (k % N1) + k / N1; }
+template <int N1, int N2>
+HD int freq_at(int p) { return p / N2 + N1 * (p % N2); }
+
+// One cell pair of the correlation spectrum.  The tile holds Z = FFT2(t + i r) for two real
+// tiles t (window) and r (chip); with T = (Z(k) + conj Z(-k)) / 2 and R = (Z(k) - conj Z(-k)) / 2i
+// the correlation spectrum is T conj R, Hermitian because the correlation is real.  a = Z(k),
+// b = Z(-k); returns 4 T conj R (the factor 4 is folded into the final scale).
+HD float2 corr_cell(float2 a, float2 b)
+{
+    const float2 t = make_float2(a.x + b.x, a.y - b.y);
+    const float2 r = make_float2(a.y + b.y, b.x - a.x);
+    return cmulc(t, r);
+}
+
+// position of -k for the frequency k held at position p (the partner of a cell in the
+// correlation spectrum)
+template <int N1, int N2>
+HD int neg_pos(int p)
+{
+    constexpr int N = N1 * N2;
+    return pos_of<N1, N2>((N - freq_at<N1, N2>(p)) % N);
+}
+
+// ---- the 2-D correlation of one tile pair -------------------------------------------------
+//
+// Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)
+// holding t + i r: the window t in the real parts, the chip r in the imaginary parts, zero
+// outside them.  Rows at and past rows_in are all zero.  neg[p] = neg_pos(p) for p < N.
+// Afterwards, for u < rows_out and v < N, Z[u][v].x holds 4 N^2 sum_ij r(i, j) t(u + i, v + j)
+// (circular indices, which never wrap for the placements of a window of at most N samples).  The
+// tasks of each phase are spread over the nt threads; sync() separates the phases
+// (__syncthreads on the device).
+template <int N1, int N2, class Sync>
+HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
+                       const int* neg, int tid, int nt, Sync sync)
+{
+    constexpr int N = N1 * N2;
+    // forward along rows: lanes take consecutive rows
+    for (int t = tid; t < rows_in * N2; t += nt) {
+        const int y = t % rows_in, n2 = t / rows_in;
+        fwd_a<N1, N2>(Z + y * RS, 1, n2, tw);
+    }
+    sync();
+    for (int t = tid; t < rows_in * N1; t += nt) {
+        const int y = t % rows_in, k1 = t / rows_in;
+        step_b<N1, N2, -1>(Z + y * RS, 1, k1);
+    }
+    sync();
+    // forward along columns: lanes take consecutive columns
+    for (int t = tid; t < N * N2; t += nt) {
+        const int x = t % N, n2 = t / N;
+        fwd_a<N1, N2>(Z + x, RS, n2, tw);
+    }
+    sync();
+    for (int t = tid; t < N * N1; t += nt) {
+        const int x = t % N, k1 = t / N;
+        step_b<N1, N2, -1>(Z + x, RS, k1);
+    }
+    sync();
+    // correlation spectrum, one thread per cell pair (k, -k)
+    for (int t = tid; t < N * N; t += nt) {
+        const int py = t / N, px = t - py * N;
+        const int qy = neg[py], qx = neg[px];
+        const int l2 = qy * N + qx;
+        if (t <= l2) {
+            const float2 a = Z[py * RS + px];
+            const float2 b = Z[qy * RS + qx];
+            const float2 c = corr_cell(a, b);
+            Z[py * RS + px] = c;
+            if (t != l2) Z[qy * RS + qx] = make_float2(c.x, -c.y);
+        }
+    }
+    sync();
+    // inverse along columns
+    for (int t = tid; t < N * N1; t += nt) {
+        const int x = t % N, k1 = t / N;
+        step_b<N1, N2, 1>(Z + x, RS, k1);
+    }
+    sync();
+    for (int t = tid; t < N * N2; t += nt) {
+        const int x = t % N, n2 = t / N;
+        inv_a<N1, N2>(Z + x, RS, n2, tw);
+    }
+    sync();
+    // inverse along the rows that hold placements
+    for (int t = tid; t < rows_out * N1; t += nt) {
+        const int y = t % rows_out, k1 = t / rows_out;
+        step_b<N1, N2, 1>(Z + y * RS, 1, k1);
+    }
+    sync();
+    for (int t = tid; t < rows_out * N2; t += nt) {
+        const int y = t % rows_out, n2 = t / rows_out;
+        inv_a<N1, N2>(Z + y * RS, 1, n2, tw);
+    }
+    sync();
+}
+
+}  // namespace fft
+}  // namespace ampcor_b200

@@ -73,6 +73,8 @@ struct PairSource {
     const float2* tgt_base;
     const long long* tgt_off;
     long long tgt_stride;
+    long long ref_count;  // samples behind ref_base (the raster or the arena)
+    long long tgt_count;
 };
 
 // coarse result of one pair
@@ -173,5 +175,66 @@ __global__ void zoom_kernel(const float* gam, long long pair0, long long pairs,
                             const CoarseOut* coarse, const float* coarse_peak, const FineOut* fout,
                             int margin, int refine_factor, int refine_margin, int ref_compat,
                             float2* offsets, PairDiag* diag);
+
+// spectral form: FFT correlation of one tile pair per CTA (512 threads, one CTA per SM).  The
+// N x N tile (N = N1 N2 >= W, row stride RS = N + 1 complex samples) holds the window in its real
+// parts and the zero-mean chip in its imaginary parts.
+struct SpecGeom {
+    int R, W, C;      // chip, window, placements per axis
+    int N, N1, N2;    // transform length and its two register radices
+    int RS;           // tile row stride (complex samples)
+    int off_z, off_tw, off_neg, off_red;  // shared-memory byte offsets
+    int smem_bytes;
+};
+
+// FP64 placement statistics of one surface per CTA (512 threads, two CTAs per SM): column sums
+// over R rows for a slice of SU placement rows at a time (nb blocks of placement rows per
+// column), then prefix sums along each row
+struct BoxGeom {
+    int R, W, C;
+    int SU;        // placement rows per slice
+    int nb;        // blocks of placement rows per column
+    int VS;        // row stride of the column-sum slices (doubles), W + 1
+    int smem_bytes;
+};
+
+// float amplitude tiles of chunk-local pair b (global pair pair0 + b): at base + off[pair0 + b]
+// when off is given, else at base + b * step; rows stride apart
+struct SpecSource {
+    const float* chip;
+    long long chip_stride;
+    const long long* chip_off;
+    long long chip_step;
+    const float* win;
+    long long win_stride;
+    const long long* win_off;
+    long long win_step;
+};
+
+// what a spectral correlation writes: stage 0 the coarse maximum (nudged corners, peak and
+// optionally the surface), stage 1 the refined maximum and the refined surface for the zoom
+struct SpecOut {
+    int stage;
+    int m;  // refinement margin (the nudge)
+    CoarseOut* coarse;
+    float* coarse_peak;
+    FineOut* fine;
+    float* gam;       // chunk-local refined surfaces (stage 1)
+    float* surfaces;  // optional, indexed by global pair
+};
+
+// |z| of every sample of a complex array (n samples)
+__global__ void detect_kernel(const float2* src, long long n, float* dst);
+__global__ void box_stats_kernel(SpecSource s, long long pair0, long long pairs,
+                                 const long long* valid, BoxGeom g, float* inv);
+
+// the transform lengths that are compiled, with their radices
+bool spec_radices(int n, int& n1, int& n2);
+int spec_next_length(int w);
+// allow every instantiation its shared memory; call once per device
+cudaError_t spec_set_smem_limits();
+cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
+                        long long pair0, long long pairs, const long long* valid, const float* inv,
+                        const float2* tw, SpecOut out);
 
 }  // namespace ampcor_b200

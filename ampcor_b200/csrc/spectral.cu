@@ -1,0 +1,418 @@
+// sm_100a kernels of the spectral correlation form.
+//
+// The numerator surface of a tile pair, sum_ij r'(i, j) t(u + i, v + j) over every placement, is
+// a 2-D correlation; the reference evaluates it as a direct sum (correlate.cu:69-135), which costs
+// C^2 R^2 multiply-adds per pair.  Here one CTA per pair does it with FFTs in shared memory:
+// the window t (real parts) and the zero-mean chip r' (imaginary parts) share one N x N complex
+// tile (N >= W, so no placement wraps around), one forward 2-D transform gives both spectra, their
+// product T conj(R) is formed in place and one inverse transform (pruned to the C placement rows)
+// returns the numerators.  About 20x fewer operations than the direct sum at the production
+// geometry (64^2 chips, 128^2 windows).
+//
+// Around it: the amplitudes of each raster are detected once (detect_kernel; neighbouring
+// windows overlap, so every sample is shared by many pairs), the FP64 placement statistics of a
+// chunk come from their own kernel (box_stats_kernel, two CTAs per SM, every thread busy), and the
+// correlation kernel takes float amplitudes through asynchronous copies.
+//
+// Accuracy.  The window is centred on its mean before the transform (sum r' = 0, so the
+// numerators keep their value) and the twiddles are correctly rounded, which keeps the transform
+// error of a normalised correlation near 1e-7; the plain form's FP32 direct sums land in the same
+// range.  Where a nearly flat box would magnify the transform error, the numerator is recomputed
+// as a direct sum (spec_surface).
+#include "fft.cuh"
+#include "kernels.cuh"
+#include "tile_common.cuh"
+
+namespace ampcor_b200 {
+
+namespace {
+
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
+// two block-wide FP64 sums in a fixed order (one pair of barriers); every thread gets both
+__device__ void block_sum2(double& a, double& b, double* red)
+{
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[2 * warp] = a;
+        red[2 * warp + 1] = b;
+    }
+    __syncthreads();
+    a = 0.0;
+    b = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        a += red[2 * w];
+        b += red[2 * w + 1];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ const float* spec_chip(const SpecSource& s, long long pair0, int b)
+{
+    return s.chip + (s.chip_off ? s.chip_off[pair0 + b] : (long long)b * s.chip_step);
+}
+
+__device__ __forceinline__ const float* spec_win(const SpecSource& s, long long pair0, int b)
+{
+    return s.win + (s.win_off ? s.win_off[pair0 + b] : (long long)b * s.win_step);
+}
+
+// The transform's error on a numerator is a small multiple of eps |r'| |t'| (|.|: Euclidean norms
+// of the zero-mean chip and the centred window; below 1.4e-7 |r'| |t'| over the compiled lengths
+// in host runs against FP64 sums), so its error on gamma is bounded by kSpecErr |t'| / sigma_box.
+// Where a box is nearly flat that bound grows; a placement whose bound exceeds kSpecTol has its
+// numerator recomputed as a direct FP32 sum whenever its value matters (it could be the maximum,
+// or the surface is returned).  Speckle never comes near the bound (|t'| / sigma_box is about
+// W / R); zero-padded or masked windows do.
+constexpr float kSpecErr = 1e-6f;
+constexpr float kSpecTol = 4e-6f;
+
+// Normalised surface -> first maximum (valid in every thread); optional copies of the surface.
+// The surface is built in the imaginary parts of the placement rows of the tile.
+__device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const float* __restrict__ inv,
+                             float inv_sigma, double mean_c, float tnorm, const float* chip,
+                             long long cs, const float* win, long long ws, float* out1, float* out2,
+                             float& bv, int& bi)
+{
+    const int C = g.C, RS = g.RS, R = g.R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float scale = (float)(1.0 / (4.0 * (double)g.N * (double)g.N));
+    const float ebox = kSpecErr * tnorm;
+    bv = -INFINITY;
+    bi = INT_MAX;
+    int flagged = 0;
+    for (int u = warp; u < C; u += kWarps) {
+        for (int v = lane; v < C; v += 32) {
+            const int idx = u * C + v;
+            float2* z = Z + u * RS + v;
+            const float inv_box = __ldg(inv + idx);
+            const float gv = z->x * scale * inv_box * inv_sigma;
+            z->y = gv;
+            if (ebox * inv_box > kSpecTol)
+                flagged = 1;
+            else
+                better(bv, bi, gv, idx);
+        }
+    }
+    block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
+    if (__syncthreads_or(flagged)) {
+        // direct FP32 numerators where the transform's bound is loose and the value matters: one
+        // warp per placement, lanes across the chip columns
+        const bool all = out1 || out2;
+        float wv = -INFINITY;
+        int wi = INT_MAX;
+        for (int idx = warp; idx < C * C; idx += kWarps) {
+            const float inv_box = __ldg(inv + idx);
+            const float e = ebox * inv_box;
+            const int u = idx / C, v = idx - u * C;
+            float* gp = &Z[u * RS + v].y;
+            if (!(e > kSpecTol) || !(all || *gp + e >= bv)) continue;
+            float acc = 0.0f;
+            for (int i = 0; i < R; ++i)
+                for (int j = lane; j < R; j += 32) {
+                    const float rp = (float)((double)__ldg(chip + i * cs + j) - mean_c);
+                    acc = fmaf(rp, __ldg(win + (u + i) * ws + v + j), acc);
+                }
+            const double num = warp_sum((double)acc);
+            const float gv = (float)num * inv_box * inv_sigma;
+            __syncwarp();
+            if (lane == 0) *gp = gv;
+            better(wv, wi, gv, idx);
+        }
+        // every flagged placement that could win has its exact value now; the others stay below
+        // the unflagged maximum
+        better(bv, bi, wv, wi);
+        block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
+    }
+    if (out1 || out2) {
+        for (int u = warp; u < C; u += kWarps) {
+            for (int v = lane; v < C; v += 32) {
+                const float gv = Z[u * RS + v].y;
+                if (out1) out1[u * C + v] = gv;
+                if (out2) out2[u * C + v] = gv;
+            }
+        }
+    }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(kThreads, 1)
+spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
+            const float* inv, const float2* tw_g, SpecOut out)
+{
+    extern __shared__ __align__(16) unsigned char ssm[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (valid[p] < 0) {
+        if (out.stage == 0 && tid == 0) {
+            out.coarse[p] = CoarseOut{-1, -1, -1, -1};
+            out.coarse_peak[p] = NAN;
+        }
+        return;
+    }
+    constexpr int N = N1 * N2;
+    const int RS = g.RS, W = g.W, R = g.R, C = g.C;
+    float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
+    float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
+    int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
+    double* red = reinterpret_cast<double*>(ssm + g.off_red);
+    float* Zf = reinterpret_cast<float*>(Z);
+    const float* chip = spec_chip(src, pair0, blockIdx.x);
+    const float* win = spec_win(src, pair0, blockIdx.x);
+    const long long cs = src.chip_stride, ws = src.win_stride;
+
+    // window amplitudes -> real parts, chip amplitudes -> imaginary parts (4-byte asynchronous
+    // copies, all in flight at once), zeros elsewhere
+    for (int y = warp; y < N; y += kWarps) {
+        float* zr = Zf + 2 * y * RS;
+        for (int x = lane; x < N; x += 32) {
+            if (y < W && x < W)
+                cp_async4(zr + 2 * x, win + y * ws + x);
+            else
+                zr[2 * x] = 0.0f;
+            if (y < R && x < R)
+                cp_async4(zr + 2 * x + 1, chip + y * cs + x);
+            else
+                zr[2 * x + 1] = 0.0f;
+        }
+    }
+    for (int k = tid; k < N; k += kThreads) {
+        tw[k] = __ldg(tw_g + k);
+        neg[k] = fft::neg_pos<N1, N2>(k);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // chip mean (FP64) and window mean; then the zero-mean chip with 1/|r'| (refStats.cu:118-302,
+    // FP64 accumulation) and the centred window with |t'|
+    double sc = 0.0, sw = 0.0;
+    for (int y = warp; y < W; y += kWarps) {
+        const float2* zr = Z + y * RS;
+        for (int x = lane; x < W; x += 32) {
+            const float2 z = zr[x];
+            sw += z.x;
+            if (y < R && x < R) sc += z.y;
+        }
+    }
+    block_sum2(sc, sw, red);
+    const double mean_c = sc / ((double)R * (double)R);
+    const float mean_w = (float)(sw / ((double)W * (double)W));
+    double ss = 0.0, st = 0.0;
+    for (int y = warp; y < W; y += kWarps) {
+        float2* zr = Z + y * RS;
+        for (int x = lane; x < W; x += 32) {
+            float2 z = zr[x];
+            z.x -= mean_w;
+            st += (double)z.x * (double)z.x;
+            if (y < R && x < R) {
+                z.y = (float)((double)z.y - mean_c);
+                ss += (double)z.y * (double)z.y;
+            }
+            zr[x] = z;
+        }
+    }
+    block_sum2(ss, st, red);
+    const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
+
+    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, tid, kThreads, BlockSync{});
+
+    float bv;
+    int bi;
+    const float* inv_b = inv + (long long)blockIdx.x * C * C;
+    float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
+    float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
+    spec_surface(Z, red, g, inv_b, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam,
+                 surf, bv, bi);
+    if (tid == 0) {
+        const int u = bi / C, v = bi - u * C;
+        if (out.stage == 0) {
+            // nudge.cu:107-140 (argument roles from nudge.cu:57: old = W, new = R + 2m)
+            const int m = out.m;
+            const int E = R + 2 * m;
+            int left = v - m;
+            if (left < 0) left = 0;
+            if (left + E > W) left = W - E;
+            int top = u - m;
+            if (top < 0) top = 0;
+            if (top + E > W) top = W - E;
+            out.coarse[p] = CoarseOut{u, v, top, left};
+            out.coarse_peak[p] = bv;
+        } else {
+            out.fine[p] = FineOut{u, v, bv, 0.0f};
+        }
+    }
+}
+
+// transform lengths: N, N1, N2 (N1 N2 = N)
+#define AMPCOR_SPEC_LENGTHS(X) \
+    X(16, 4, 4)                \
+    X(24, 4, 6)                \
+    X(32, 4, 8)                \
+    X(40, 5, 8)                \
+    X(48, 6, 8)                \
+    X(64, 8, 8)                \
+    X(80, 8, 10)               \
+    X(96, 8, 12)               \
+    X(120, 8, 15)              \
+    X(128, 8, 16)              \
+    X(144, 12, 12)             \
+    X(160, 10, 16)
+
+}  // namespace
+
+__global__ void detect_kernel(const float2* __restrict__ src, long long n, float* __restrict__ dst)
+{
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 4 * step) {
+        float2 z[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long j = i + k * step;
+            z[k] = j < n ? __ldg(src + j) : make_float2(0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long j = i + k * step;
+            if (j < n) dst[j] = amp_of(z[k]);
+        }
+    }
+}
+
+// 1/sqrt(sum_box t^2 - (sum_box t)^2 / R^2) of every placement of a chunk-local pair (0 for a flat
+// box): the FP64 summed-area statistics of tgtStats.cu:139-162 and sat.cu:81-149, evaluated as
+// column sums slid down the window (FP64) and prefix sums along the placement rows.  The window
+// is read from L2 / HBM as it is; only the column sums live in shared memory.
+__global__ void __launch_bounds__(kThreads, 2)
+box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long* valid, BoxGeom g,
+                 float* inv)
+{
+    extern __shared__ __align__(16) double bsm[];
+    if (blockIdx.x >= pairs) return;
+    if (valid[pair0 + blockIdx.x] < 0) return;
+    const float* win = spec_win(s, pair0, blockIdx.x);
+    const long long ws = s.win_stride;
+    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* V1 = bsm;
+    double* V2 = bsm + SU * VS;
+    float* out = inv + (long long)blockIdx.x * C * C;
+    const double cells = (double)R * (double)R;
+    for (int u0 = 0; u0 < C; u0 += SU) {
+        const int nu = min(SU, C - u0);
+        const int B = (nu + nb - 1) / nb;
+        for (int t = tid; t < W * nb; t += kThreads) {
+            const int x = t % W, ub = t / W;
+            const int ua = u0 + ub * B, ue = min(ua + B, u0 + nu);
+            if (ua >= ue) continue;
+            const float* col = win + x;
+            double a1[4] = {0.0, 0.0, 0.0, 0.0}, a2[4] = {0.0, 0.0, 0.0, 0.0};
+            int i = 0;
+            for (; i + 4 <= R; i += 4) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const double tv = __ldg(col + (long long)(ua + i + k) * ws);
+                    a1[k] += tv;
+                    a2[k] += tv * tv;
+                }
+            }
+            for (; i < R; ++i) {
+                const double tv = __ldg(col + (long long)(ua + i) * ws);
+                a1[0] += tv;
+                a2[0] += tv * tv;
+            }
+            double s1 = (a1[0] + a1[1]) + (a1[2] + a1[3]);
+            double s2 = (a2[0] + a2[1]) + (a2[2] + a2[3]);
+            for (int u = ua; u < ue; ++u) {
+                V1[(u - u0) * VS + x] = s1;
+                V2[(u - u0) * VS + x] = s2;
+                if (u + 1 < ue) {
+                    const double a = __ldg(col + (long long)(u + R) * ws);
+                    const double b = __ldg(col + (long long)u * ws);
+                    s1 += a - b;
+                    s2 += a * a - b * b;
+                }
+            }
+        }
+        __syncthreads();
+        for (int r = warp; r < nu; r += kWarps) {
+            warp_prefix(V1 + r * VS, W);
+            warp_prefix(V2 + r * VS, W);
+            __syncwarp();
+            for (int v = lane; v < C; v += 32) {
+                const double b1 = V1[r * VS + v + R] - V1[r * VS + v];
+                const double b2 = V2[r * VS + v + R] - V2[r * VS + v];
+                const float var = (float)(b2 - b1 * b1 / cells);
+                out[(u0 + r) * C + v] = var > 0.0f ? __frsqrt_rn(var) : 0.0f;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+bool spec_radices(int n, int& n1, int& n2)
+{
+#define AMPCOR_SPEC_CASE(NN, A, B) \
+    if (n == NN) {                 \
+        n1 = A;                    \
+        n2 = B;                    \
+        return true;               \
+    }
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return false;
+}
+
+int spec_next_length(int w)
+{
+#define AMPCOR_SPEC_CASE(NN, A, B) \
+    if (w <= NN) return NN;
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return 0;
+}
+
+cudaError_t spec_set_smem_limits()
+{
+    const int limit = 227 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(box_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+#define AMPCOR_SPEC_CASE(NN, A, B) \
+    if (e == cudaSuccess)          \
+        e = cudaFuncSetAttribute(spec_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return e;
+}
+
+cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
+                        long long pair0, long long pairs, const long long* valid, const float* inv,
+                        const float2* tw, SpecOut out)
+{
+#define AMPCOR_SPEC_CASE(NN, A, B)                                                              \
+    if (g.N == NN) {                                                                            \
+        spec_kernel<A, B><<<blocks, kThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g, \
+                                                                  inv, tw, out);                \
+        return cudaGetLastError();                                                              \
+    }
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ampcor_b200

@@ -1,0 +1,181 @@
+// Device helpers shared by the FP32 kernels of the plain and spectral forms (512-thread CTAs):
+// amplitudes, fixed-order block reductions, the reference's first-maximum order and the FP64
+// placement statistics.
+#pragma once
+
+#include "kernels.cuh"
+
+#include <limits.h>
+#include <math.h>
+
+namespace ampcor_b200 {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// |z| as the reference CPU path computes it (float std::abs of complex<float>): the FP64
+// square root of the exactly formed FP64 sum of squares, rounded to float
+__device__ __forceinline__ float amp_of(float2 z)
+{
+    const double re = z.x, im = z.y;
+    return (float)sqrt(re * re + im * im);
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// block-wide FP64 sum in a fixed order; every thread gets the same value
+__device__ double block_sum(double v, double* red)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) s += red[w];
+    __syncthreads();
+    return s;
+}
+
+// (value, index) order of the reference argmax (maxcor.cu:114-126): the first cell, in row-major
+// order, holding the largest value
+__device__ __forceinline__ void better(float& bv, int& bi, float v, int i)
+{
+    if (v > bv || (v == bv && i < bi)) {
+        bv = v;
+        bi = i;
+    }
+}
+
+__device__ void block_argmax(float& bv, int& bi, float* redf, int* redi)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        better(bv, bi, ov, oi);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        redf[warp] = bv;
+        redi[warp] = bi;
+    }
+    __syncthreads();
+    bv = redf[0];
+    bi = redi[0];
+    for (int w = 1; w < kWarps; ++w) better(bv, bi, redf[w], redi[w]);
+    __syncthreads();
+}
+
+template <int NT>
+__device__ void block_argmax_n(float& bv, int& bi, float* redf, int* redi)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        better(bv, bi, ov, oi);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        redf[warp] = bv;
+        redi[warp] = bi;
+    }
+    __syncthreads();
+    bv = redf[0];
+    bi = redi[0];
+    for (int w = 1; w < NT / 32; ++w) better(bv, bi, redf[w], redi[w]);
+    __syncthreads();
+}
+
+// exclusive prefix sum of row[0..n) written in place, with the total in row[n] (one warp)
+__device__ void warp_prefix(double* row, int n)
+{
+    const int lane = threadIdx.x & 31;
+    const int per = (n + 31) / 32;
+    const int beg = min(lane * per, n), end = min(beg + per, n);
+    double local = 0.0;
+    for (int k = beg; k < end; ++k) local += row[k];
+    double incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    double run = __shfl_up_sync(kFull, incl, 1);
+    if (lane == 0) run = 0.0;
+    for (int k = beg; k < end; ++k) {
+        const double v = row[k];
+        row[k] = run;
+        run += v;
+    }
+    if (end == n && beg < n) row[n] = run;
+}
+
+// 1/sqrt(sum_box t^2 - (sum_box t)^2 / R^2) for every placement, 0 for a flat box.
+// FP64 column sums slide down the window; each chunk of kStatRows placement rows is turned into
+// box sums by a prefix sum along the row (the FP64 summed-area table of tgtStats.cu:139-162 and
+// sat.cu:81-149, evaluated in slices so that it fits beside the tiles).
+// (XS: the column stride of the window in floats; S: its row stride)
+template <int XS>
+__device__ void window_stats_xs(const float* win, int S, int W, int R, int C, int SR, float* inv,
+                                double* vbuf)
+{
+    const int tid = threadIdx.x, warp = tid >> 5;
+    double* V1 = vbuf;
+    double* V2 = vbuf + SR * (W + 1);
+    double s1 = 0.0, s2 = 0.0;
+    if (tid < W) {
+        for (int i = 0; i < R; ++i) {
+            const double t = win[i * S + tid * XS];
+            s1 += t;
+            s2 += t * t;
+        }
+    }
+    const double cells = (double)R * (double)R;
+    for (int u0 = 0; u0 < C; u0 += SR) {
+        const int nrows = min(SR, C - u0);
+        if (tid < W) {
+            for (int r = 0; r < nrows; ++r) {
+                const int u = u0 + r;
+                V1[r * (W + 1) + tid] = s1;
+                V2[r * (W + 1) + tid] = s2;
+                if (u + 1 < C) {
+                    const double a = win[(u + R) * S + tid * XS], b = win[u * S + tid * XS];
+                    s1 += a - b;
+                    s2 += a * a - b * b;
+                }
+            }
+        }
+        __syncthreads();
+        if (warp < nrows) {
+            warp_prefix(V1 + warp * (W + 1), W);
+            warp_prefix(V2 + warp * (W + 1), W);
+        }
+        __syncthreads();
+        for (int idx = tid; idx < nrows * C; idx += kThreads) {
+            const int r = idx / C, v = idx - r * C;
+            const double* p1 = V1 + r * (W + 1);
+            const double* p2 = V2 + r * (W + 1);
+            const double b1 = p1[v + R] - p1[v];
+            const double b2 = p2[v + R] - p2[v];
+            const double var = b2 - b1 * b1 / cells;
+            inv[(u0 + r) * C + v] = var > 0.0 ? (float)(1.0 / sqrt(var)) : 0.0f;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void window_stats(const float* win, const NccGeom& g, float* inv,
+                                             double* vbuf)
+{
+    window_stats_xs<1>(win, g.S, g.W, g.R, g.C, g.stat_rows, inv, vbuf);
+}
+
+}  // namespace
+}  // namespace ampcor_b200

@@ -16,6 +16,9 @@ import numpy as np
 
 from . import _lib
 
+# correlation forms, indexed by the value ampcor_form returns
+FORMS = ("plain", "tensor", "spectral")
+
 
 class Error(Exception):
     """Raised when the correlator library reports a failure (the extension's ``Error``,
@@ -65,8 +68,9 @@ class Worker:
         c, r, z = c_int32(), c_int32(), c_int32()
         self._lib.ampcor_surface_dims(handle, byref(c), byref(r), byref(z))
         self.coarse_dim, self.refined_dim, self.zoomed_dim = c.value, r.value, z.value
-        # "tensor": bf16x3 split products on the tensor cores; "plain": FP32 FMA
-        self.form = "tensor" if self._lib.ampcor_form(handle) == 1 else "plain"
+        # "spectral": FFT correlation in shared memory; "tensor": bf16x3 split products on the
+        # tensor cores; "plain": FP32 FMA direct sums
+        self.form = FORMS[self._lib.ampcor_form(handle)]
 
     # lifetime
     def close(self):
@@ -130,11 +134,11 @@ class Worker:
         return c.value, r.value, f.value, n.value
 
     def configure(self, form=None, chunk=None):
-        """Select the form ("tensor" or "plain") and the refinement chunk (pairs)."""
-        f = {None: -1, "plain": 0, "tensor": 1}[form]
+        """Select the form ("spectral", "tensor" or "plain") and the refinement chunk (pairs)."""
+        f = -1 if form is None else FORMS.index(form)
         _check(self._lib, self._handle,
                self._lib.ampcor_configure(self._handle, f, int(chunk or 0)))
-        self.form = "tensor" if self._lib.ampcor_form(self._handle) == 1 else "plain"
+        self.form = FORMS[self._lib.ampcor_form(self._handle)]
 
     @property
     def chunk(self):

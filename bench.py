@@ -238,7 +238,7 @@ def run_b200(args):
     if not args.no_tune:
         from ampcor_b200.autotune import tune
 
-        forms = ("plain",) if args.plain else ("tensor", "plain")
+        forms = ("plain",) if args.plain else ("spectral", "tensor", "plain")
         tuned = tune(worker, ref, tgt, ulhc, forms=forms, use_cache=False)
 
     def step():
@@ -317,11 +317,15 @@ def run_b200(args):
             "refinement": 4.0 * (f * f - 1) * (w.chip ** 3 + E ** 3),
         }
         names = {
-            "coarse_correlation": "tc_coarse_kernel" if worker.form == "tensor" else "coarse_kernel",
-            "fine_correlation": "tc_fine_kernel" if worker.form == "tensor" else "fine_kernel",
+            "coarse_correlation": {"tensor": "tc_coarse_kernel", "spectral": "spec_kernel (coarse)"}
+            .get(worker.form, "coarse_kernel"),
+            "fine_correlation": {"tensor": "tc_fine_kernel", "spectral": "spec_kernel (fine)"}
+            .get(worker.form, "fine_kernel"),
             "refinement": "refine_kernel",
-            "coarse_statistics": "window_stats_cplx_kernel",
-            "fine_statistics": "window_stats_real_kernel",
+            "coarse_statistics": {"spectral": "detect_kernel + box_stats_kernel (coarse)"}
+            .get(worker.form, "window_stats_cplx_kernel"),
+            "fine_statistics": {"spectral": "box_stats_kernel (fine)"}
+            .get(worker.form, "window_stats_real_kernel"),
             "zoom": "zoom_kernel",
         }
         top = max(flop_pair, key=lambda k: kt[k][0])

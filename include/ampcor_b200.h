@@ -32,7 +32,8 @@ extern "C" {
                                       subtracts the refine margin a second time
                                       (lib/libampcor_cuda/correlators/offsets.cu:124-125) */
 #define AMPCOR_FLAG_PLAIN_FP32 2u  /* correlate with FP32 fused multiply-adds (the plain form)
-                                      instead of bf16x3 split products on the tensor cores */
+                                      instead of FFTs (the spectral form) or bf16x3 split
+                                      products on the tensor cores */
 
 typedef struct ampcor_handle ampcor_handle;
 
@@ -171,19 +172,20 @@ int ampcor_correlate_noalloc(const ampcor_params* params, const ampcor_job* job,
 
 /* Device time (ms) and launch count per kernel kind since profiling was switched on or last read:
    [0] coarse correlation, [1] refinement, [2] fine correlation, [3] coarse placement statistics,
-   [4] fine placement statistics, [5] zoom ([3]-[5] run in the tensor-core form only); resets the
-   counters.  No reference counterpart. */
+   [4] fine placement statistics, [5] zoom ([3]-[4] run in the tensor-core form only, [5] in the
+   tensor-core and spectral forms); resets the counters.  No reference counterpart. */
 int ampcor_kernel_times(ampcor_handle* handle, double* ms, uint64_t* launches);
 
-/* 1 if the worker correlates on the tensor cores (bf16x3 split products), 0 for the plain FP32
-   form, -1 for a NULL handle.  The tensor-core form is the default wherever the geometry allows
-   it (at most 128 placements per axis); AMPCOR_FLAG_PLAIN_FP32 selects the plain form.  No
-   reference counterpart. */
+/* The worker's correlation form: 2 spectral (FFT correlation in shared memory), 1 tensor cores
+   (bf16x3 split products), 0 plain FP32 direct sums; -1 for a NULL handle.  The spectral form is
+   the default wherever the geometry allows it (windows of at most 160 samples, refined windows
+   included), then the tensor-core form (at most 128 placements per axis);
+   AMPCOR_FLAG_PLAIN_FP32 selects the plain form.  No reference counterpart. */
 int ampcor_form(const ampcor_handle* handle);
 
-/* Choose the correlation form (form: 1 tensor cores, 0 plain FP32, -1 unchanged) and the number
-   of pairs refined per chunk (chunk: 0 unchanged), as an autotuner does.  Waits for the worker's
-   stream.  No reference counterpart. */
+/* Choose the correlation form (form: 2 spectral, 1 tensor cores, 0 plain FP32, -1 unchanged) and
+   the number of pairs refined per chunk (chunk: 0 unchanged), as an autotuner does.  Waits for
+   the worker's stream.  No reference counterpart. */
 int ampcor_configure(ampcor_handle* handle, int form, uint64_t chunk);
 
 /* The number of pairs refined per chunk. */

@@ -27,7 +27,7 @@ PEAK_RTOL = 1e-5
 SURF_ATOL = 2e-5
 
 
-FORMS = ["tensor", "plain"]
+FORMS = ["spectral", "tensor", "plain"]
 
 
 def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor"):
@@ -35,6 +35,8 @@ def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor"):
     worker = Worker(pairs=len(ulhc), chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
                     zoom_factor=w.zoom_factor, plain=(form == "plain"))
+    if worker.form != form:
+        worker.configure(form)
     assert worker.form == form
     dev = torch.device("cuda:0")
     ref = torch.from_numpy(w.ref).to(dev)
@@ -172,7 +174,7 @@ def test_host_path_matches_device_path():
     worker = Worker(pairs=w.pairs, chip=(32, 32), window=(48, 48), refine_factor=2,
                     refine_margin=4, zoom_factor=4)
     off, diag = worker.correlate(w.ref, w.tgt, w.ulhc, diag=True)
-    dev = run_device(w)
+    dev = run_device(w, form=worker.form)
     assert np.array_equal(off, dev["offsets"])
     assert np.array_equal(diag, dev["diag"])
 
@@ -187,7 +189,7 @@ def test_extension_mirror_matches_raster_path():
     offsets = ampcor_cuda.adjust(worker)
     assert isinstance(offsets, tuple) and len(offsets) == w.pairs
     assert all(isinstance(o, tuple) and len(o) == 2 for o in offsets)
-    dev = run_device(w)
+    dev = run_device(w, form=ampcor_cuda._worker(worker).form)
     assert np.array_equal(np.array(offsets, np.float32), dev["offsets"])
 
 
@@ -218,12 +220,13 @@ def test_out_of_bounds_pair_reports_and_is_nan():
     assert np.isnan(o[2]).all() and np.isfinite(o[[0, 1, 3]]).all()
 
 
-def test_tensor_and_plain_forms_agree():
-    # the two forms on the same pairs: same integer and sub-pixel cells except near-ties,
-    # surfaces within the parity tolerance of each other
+@pytest.mark.parametrize("form", ["tensor", "spectral"])
+def test_forms_agree_with_plain(form):
+    # a form and the plain form on the same pairs: same integer and sub-pixel cells except
+    # near-ties, surfaces within the parity tolerance of each other
     w = synth.production_4096()
     idx = _subset(w, 256, seed=3)
-    t = run_device(w, ulhc=w.ulhc[idx], surfaces=True, form="tensor")
+    t = run_device(w, ulhc=w.ulhc[idx], surfaces=True, form=form)
     p = run_device(w, ulhc=w.ulhc[idx], surfaces=True, form="plain")
     np.testing.assert_allclose(t["coarse"], p["coarse"], atol=SURF_ATOL, rtol=0)
     np.testing.assert_allclose(t["refined"], p["refined"], atol=SURF_ATOL, rtol=0)
