@@ -20,8 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CC = "/usr/bin/gcc"
 
-CUDA_SOURCES = ["kernels.cu", "tc_ncc.cu", "spectral.cu", "capi.cu"]
-CUDA_HEADERS = ["kernels.cuh", "tile_common.cuh", "fft.cuh", os.path.join("..", "..", "include", "ampcor_b200.h")]
+CUDA_SOURCES = ["kernels.cu", "tc_ncc.cu", "tc_zoom.cu", "spectral.cu", "capi.cu"]
+CUDA_HEADERS = ["kernels.cuh", "tile_common.cuh", "fft.cuh", "tcgen05.cuh", os.path.join("..", "..", "include", "ampcor_b200.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -264,6 +264,81 @@ bool plan_box(int R, int W, BoxGeom& g, std::string& err)
     return true;
 }
 
+// the tensor-core zoom: operand planes, accumulator parts and row tiles; false when Zm does not fit
+// (more than 512 accumulator columns or more shared memory than a CTA has)
+bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
+{
+    std::memset(&g, 0, sizeof(g));
+    g.Cf = Cf;
+    g.z = z;
+    g.Z = Cf * z;
+    const int KP = (Cf + 7) / 8 * 8;
+    g.KC = KP / 4;
+    g.NG = (Cf + 15) / 16 * 16;
+    if (g.NG > 64) return false;
+    const int zq = (g.Z + 15) / 16 * 16;
+    g.nparts = zq > 256 ? 2 : 1;
+    g.npart = ((zq + g.nparts - 1) / g.nparts + 15) / 16 * 16;
+    if (g.npart > 256) return false;
+    const int full = g.Z / 128, rem = g.Z - 128 * full;
+    g.mtiles = full + (rem ? 1 : 0);
+    g.last_m = (rem == 0 || rem > 64) ? 128 : 64;
+    // accumulators: Zm parts at columns 0 and 256; the tiles of T^T at columns 64 mt
+    const int cols = std::max(g.nparts == 2 ? 512 : g.npart, 64 * g.mtiles);
+    g.tmem_cols = 32;
+    while (g.tmem_cols < cols) g.tmem_cols *= 2;
+    if (g.tmem_cols > 512) return false;
+    const long rg = (long)g.KC * 128;
+    const long plane_a = (long)((g.Z + 7) / 8) * rg;
+    const long plane_b = (long)(g.nparts * g.npart / 8) * rg;
+    const long plane_g = (long)(g.NG / 8) * rg;
+    // the last row tile may read row groups past U; they must land in the next plane (U's lo
+    // plane, then the B planes)
+    const long over = (long)(128 * (g.mtiles - 1) + g.last_m - (g.Z + 7) / 8 * 8) / 8 * rg;
+    if (over > plane_b) return false;
+    long off = 0;
+    g.off_ahi = 0;
+    g.off_alo = (int)(off += plane_a);
+    g.off_bhi = (int)(off += plane_a);
+    g.off_blo = (int)(off += plane_b);
+    g.off_ghi = (int)(off += plane_b);
+    g.off_glo = (int)(off += plane_g);
+    off += plane_g;
+    g.off_bar = (int)off;
+    off += 16;
+    g.off_misc = (int)off;
+    off += 128;
+    g.smem_bytes = (int)off;
+    return off <= 227L * 1024;
+}
+
+double dirichlet(int N, double d);
+
+// hi and lo tf32 planes of U (U[p][a] = D_Cf(p / z - a), an identity row for p % z == 0), rows of
+// K-major core matrices; K past Cf is zero
+std::vector<float> zoom_u_planes(const ZoomTcGeom& g)
+{
+    const int rows = (g.Z + 7) / 8 * 8;
+    const size_t plane = (size_t)rows * g.KC * 4;
+    std::vector<float> out(2 * plane, 0.0f);
+    for (int p = 0; p < g.Z; ++p)
+        for (int a = 0; a < g.Cf; ++a) {
+            const int s = p % g.z, b = p / g.z;
+            const float u = s == 0 ? (b == a ? 1.0f : 0.0f) : (float)dirichlet(g.Cf, (double)p / g.z - a);
+            // round to tf32: nearest, ties away from zero
+            uint32_t bits;
+            std::memcpy(&bits, &u, 4);
+            bits = (bits + 0x1000u) & 0xFFFFE000u;
+            float hi;
+            std::memcpy(&hi, &bits, 4);
+            const float lo = u - hi;
+            const size_t off = (size_t)((p / 8) * g.KC + a / 4) * 32 + (p % 8) * 4 + a % 4;
+            out[off] = hi;
+            out[plane + off] = lo;
+        }
+    return out;
+}
+
 // exp(-2 pi i m / N), m < N, rounded from FP64
 std::vector<float> spec_twiddle_table(int N)
 {
@@ -360,6 +435,10 @@ struct ampcor_handle {
     int form = 0;
     SpecGeom spc{}, spf{};
     BoxGeom bxc{}, bxf{};
+    // tensor-core zoom (both the tensor-core and the spectral forms), when Zm fits
+    bool zoom_tc = false;
+    ZoomTcGeom ztc{};
+    float* d_zoom_uhl = nullptr;
     float* d_tw_c = nullptr;
     float* d_tw_f = nullptr;
     // amplitude rasters of the spectral form (reference and secondary, one allocation)
@@ -550,6 +629,25 @@ void drop_marks(ampcor_handle* h)
     for (cudaEvent_t e : seen) cudaEventDestroy(e);
 }
 
+// the zoom of a chunk: tensor cores where Zm fits, else the FP32 kernel
+int launch_zoom(ampcor_handle* h, long long c0, unsigned n, const PairSource& src, float2* offsets,
+                PairDiag* diag, cudaStream_t st)
+{
+    const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
+    if (h->zoom_tc) {
+        const unsigned blocks = std::min<unsigned>(n, 148u);
+        tc_zoom_kernel<<<blocks, 256, h->ztc.smem_bytes, st>>>(
+            h->d_gam, c0, n, src.ref_off, h->ztc, h->d_zoom_uhl, h->d_coarse, h->d_coarse_peak,
+            h->d_fine_out, h->M, h->f, h->m, compat, offsets, diag, h->d_tc_err);
+    } else {
+        zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg, h->d_zoom_ut,
+                                                  h->d_coarse, h->d_coarse_peak, h->d_fine_out, h->M,
+                                                  h->f, h->m, compat, offsets, diag);
+    }
+    CK(h, cudaGetLastError(), "launching the zoom kernel");
+    return AMPCOR_OK;
+}
+
 // tensor-core form, per chunk: coarse statistics -> coarse correlation -> refinement -> fine
 // statistics -> fine correlation -> zoom
 int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
@@ -560,7 +658,6 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
     if (rc) return rc;
     if ((rc = ensure_fine_out(h, (size_t)pairs))) return rc;
     const RealTiles rt{h->d_refined, h->refined_stride, 0, (long long)h->Rf * h->Rf};
-    const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
     for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
         cudaEvent_t a = mark(h, st);
@@ -585,12 +682,9 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
                                                           h->d_tc_err);
         cudaEvent_t f = mark(h, st);
         keep(h, 2, e, f);
-        zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg,
-                                                  h->d_zoom_ut, h->d_coarse, h->d_coarse_peak,
-                                                       h->d_fine_out, h->M, h->f, h->m, compat,
-                                                       offsets, diag);
-        keep(h, 5, f, mark(h, st));
         CK(h, cudaGetLastError(), "launching the tensor-core pipeline");
+        if ((rc = launch_zoom(h, c0, n, src, offsets, diag, st))) return rc;
+        keep(h, 5, f, mark(h, st));
     }
     return AMPCOR_OK;
 }
@@ -621,7 +715,6 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
     const SpecSource cs{amp_ref, src.ref_stride, src.ref_off, 0, amp_tgt, src.tgt_stride, src.tgt_off, 0};
     const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
-    const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
     for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
         cudaEvent_t a = mark(h, st);
@@ -651,10 +744,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
            "launching the spectral fine correlation");
         cudaEvent_t f = mark(h, st);
         keep(h, 2, e, f);
-        zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg, h->d_zoom_ut,
-                                                  h->d_coarse, h->d_coarse_peak, h->d_fine_out, h->M,
-                                                  h->f, h->m, compat, offsets, diag);
-        CK(h, cudaGetLastError(), "launching the zoom kernel");
+        if ((rc = launch_zoom(h, c0, n, src, offsets, diag, st))) return rc;
         keep(h, 5, f, mark(h, st));
     }
     return AMPCOR_OK;
@@ -756,6 +846,7 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         h->gsf = stats_layout(h->gf);
         const int Zp = (h->Z + 7) & ~7;
         h->zoom_smem = (round4(h->Cf * h->Cf) + 2 * h->Cf * Zp + 64) * 4;
+        h->zoom_tc = plan_zoom_tc(h->Cf, h->z, h->ztc) && !std::getenv("AMPCOR_ZOOM_FP32");
     }
 
     cudaError_t e = cudaSetDevice(p->device);
@@ -788,6 +879,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
                                   kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(zoom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kMaxSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(tc_zoom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxSmem)) != cudaSuccess ||
         (e = spec_set_smem_limits()) != cudaSuccess)
         return cuda_create_fail(e, "configuring kernel shared memory");
 
@@ -815,7 +908,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     if ((e = upload(h->d_chip_taps, ct)) != cudaSuccess || (e = upload(h->d_win_taps, wt)) != cudaSuccess ||
         (e = upload(h->d_zoom_taps, zt)) != cudaSuccess || (e = upload(h->d_zoom_ut, zut)) != cudaSuccess ||
         (e = upload(h->d_tw_c, spec_twiddle_table(std::max(h->spc.N, 1)))) != cudaSuccess ||
-        (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->spf.N, 1)))) != cudaSuccess)
+        (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->spf.N, 1)))) != cudaSuccess ||
+        (h->zoom_tc && (e = upload(h->d_zoom_uhl, zoom_u_planes(h->ztc))) != cudaSuccess))
         return cuda_create_fail(e, "uploading interpolation taps");
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess ||
@@ -855,6 +949,7 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_fine_out);
     cudaFree(h->d_tw_c);
     cudaFree(h->d_tw_f);
+    cudaFree(h->d_zoom_uhl);
     cudaFree(h->d_amp);
     cudaFree(h->d_tc_err);
     drop_marks(h);

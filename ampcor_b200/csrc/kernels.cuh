@@ -176,6 +176,31 @@ __global__ void zoom_kernel(const float* gam, long long pair0, long long pairs,
                             int margin, int refine_factor, int refine_margin, int ref_compat,
                             float2* offsets, PairDiag* diag);
 
+// tensor-core zoom (3xTF32): Zm = U G U^T with U the Z x Cf interpolation matrix, as
+// T^T = U G^T then Zm = U T; planes of K-major core matrices (8 rows x 16 bytes), K = Cf padded
+// to KC 16-byte chunks (KC even)
+struct ZoomTcGeom {
+    int Cf, z, Z;
+    int KC;        // 4-float chunks per operand row
+    int NG;        // rows of the G planes (Cf rounded to 16): N of the first product
+    int mtiles;    // tiles of rows (of T^T and of Zm): 128 each, the last one last_m (64 or 128)
+    int last_m;
+    int nparts;    // accumulator parts of Zm columns (1 or 2), npart columns each, 256 apart
+    int npart;
+    int tmem_cols;
+    int off_ahi, off_alo, off_bhi, off_blo, off_ghi, off_glo, off_bar, off_misc;  // smem bytes
+    int smem_bytes;
+};
+
+// zoom of the refined surfaces of a chunk on the tensor cores; same outputs as zoom_kernel.
+// uhl: the hi and lo planes of U, contiguous.  One CTA per SM walks the pairs.
+__global__ void tc_zoom_kernel(const float* gam, long long pair0, long long pairs,
+                               const long long* ref_off, ZoomTcGeom zt, const float* uhl,
+                               const CoarseOut* coarse, const float* coarse_peak,
+                               const FineOut* fout, int margin, int refine_factor,
+                               int refine_margin, int ref_compat, float2* offsets, PairDiag* diag,
+                               unsigned int* err_out);
+
 // spectral form: FFT correlation of one tile pair per CTA (512 threads, one CTA per SM).  The
 // N x N tile (N = N1 N2 >= W, row stride RS = N + 1 complex samples) holds the window in its real
 // parts and the zero-mean chip in its imaginary parts.

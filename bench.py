@@ -326,7 +326,7 @@ def run_b200(args):
             .get(worker.form, "window_stats_cplx_kernel"),
             "fine_statistics": {"spectral": "box_stats_kernel (fine)"}
             .get(worker.form, "window_stats_real_kernel"),
-            "zoom": "zoom_kernel",
+            "zoom": "tc_zoom_kernel (zoom_kernel where Zm exceeds the tensor memory)",
         }
         top = max(flop_pair, key=lambda k: kt[k][0])
         top_ms, top_n = kt[top]
