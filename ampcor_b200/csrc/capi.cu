@@ -441,6 +441,9 @@ struct ampcor_handle {
     float* d_zoom_uhl = nullptr;
     float* d_tw_c = nullptr;
     float* d_tw_f = nullptr;
+    // refinement by zero-padded FFT (spectral form): twiddles of R, f R, E and f E, in that order
+    bool refine_fft = false;
+    float* d_tw_refine = nullptr;
     // amplitude rasters of the spectral form (reference and secondary, one allocation)
     float* d_amp = nullptr;
     size_t amp_cap = 0;
@@ -728,10 +731,21 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
            "launching the spectral coarse correlation");
         cudaEvent_t c = mark(h, st);
         keep(h, 0, b, c);
-        refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
-                                                           h->d_chip_taps, h->d_win_taps,
-                                                           h->d_refined, h->refined_stride);
-        CK(h, cudaGetLastError(), "launching the refinement kernel");
+        if (h->refine_fft) {
+            const float2* tw = reinterpret_cast<const float2*>(h->d_tw_refine);
+            CK(h, launch_spec_refine(h->R, n, st, src.ref_base, src.ref_off, src.ref_stride, nullptr, c0,
+                                     n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0),
+               "launching the chip refinement");
+            CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
+                                     c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
+                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf),
+               "launching the window refinement");
+        } else {
+            refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
+                                                               h->d_chip_taps, h->d_win_taps,
+                                                               h->d_refined, h->refined_stride);
+            CK(h, cudaGetLastError(), "launching the refinement kernel");
+        }
         cudaEvent_t d = mark(h, st);
         keep(h, 1, c, d);
         box_stats_kernel<<<n, kThreads, h->bxf.smem_bytes, st>>>(fs, c0, n, src.ref_off, h->bxf, h->d_inv_f);
@@ -847,6 +861,9 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         const int Zp = (h->Z + 7) & ~7;
         h->zoom_smem = (round4(h->Cf * h->Cf) + 2 * h->Cf * Zp + 64) * 4;
         h->zoom_tc = plan_zoom_tc(h->Cf, h->z, h->ztc) && !std::getenv("AMPCOR_ZOOM_FP32");
+        int sm_c = 0, sm_w = 0;
+        h->refine_fft = spec_refine_supported(h->R, h->f, sm_c) && spec_refine_supported(h->E, h->f, sm_w) &&
+                        !std::getenv("AMPCOR_REFINE_TAPS");
     }
 
     cudaError_t e = cudaSetDevice(p->device);
@@ -911,6 +928,15 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->spf.N, 1)))) != cudaSuccess ||
         (h->zoom_tc && (e = upload(h->d_zoom_uhl, zoom_u_planes(h->ztc))) != cudaSuccess))
         return cuda_create_fail(e, "uploading interpolation taps");
+    if (h->refine_fft) {
+        std::vector<float> tw;
+        for (int n : {h->R, h->Rf, h->E, h->Wf}) {
+            const std::vector<float> t = spec_twiddle_table(n);
+            tw.insert(tw.end(), t.begin(), t.end());
+        }
+        if ((e = upload(h->d_tw_refine, tw)) != cudaSuccess)
+            return cuda_create_fail(e, "uploading refinement twiddles");
+    }
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMemset(h->d_bad, 0, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMalloc(&h->d_tc_err, sizeof(unsigned int))) != cudaSuccess ||
@@ -950,6 +976,7 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_tw_c);
     cudaFree(h->d_tw_f);
     cudaFree(h->d_zoom_uhl);
+    cudaFree(h->d_tw_refine);
     cudaFree(h->d_amp);
     cudaFree(h->d_tc_err);
     drop_marks(h);

@@ -310,6 +310,24 @@ HD int neg_pos(int p)
     return pos_of<N1, N2>((N - freq_at<N1, N2>(p)) % N);
 }
 
+// Zero padding of an N-point spectrum to F points (band-limited upsampling by F / N): the source
+// frequency of padded frequency kp and its weight.  The low half keeps its place, the high half
+// moves to the top, an even N's Nyquist bin is split in two halves (the Dirichlet kernel's
+// cos(pi d) term); w = 0 in the zero gap.
+template <int N, int F>
+HD int pad_source(int kp, float& w)
+{
+    w = 1.0f;
+    if (kp < (N + 1) / 2) return kp;
+    if (kp > F - (N + 1) / 2) return kp - (F - N);
+    if ((N & 1) == 0 && (kp == N / 2 || kp == F - N / 2)) {
+        w = 0.5f;
+        return N / 2;
+    }
+    w = 0.0f;
+    return 0;
+}
+
 // ---- the 2-D correlation of one tile pair -------------------------------------------------
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)

@@ -258,6 +258,13 @@ bool spec_radices(int n, int& n1, int& n2);
 int spec_next_length(int w);
 // allow every instantiation its shared memory; call once per device
 cudaError_t spec_set_smem_limits();
+// refinement by zero-padded FFT for an N x N tile and factor f, when compiled (smem: its bytes)
+bool spec_refine_supported(int n, int f, int& smem);
+cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
+                               const long long* off, long long stride, const CoarseOut* coarse,
+                               long long pair0, long long pairs, const long long* valid,
+                               const float2* twn, const float2* twf, float* refined,
+                               long long refined_stride, long long out_off);
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
                         long long pair0, long long pairs, const long long* valid, const float* inv,
                         const float2* tw, SpecOut out);

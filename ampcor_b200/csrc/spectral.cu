@@ -37,6 +37,12 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
+__device__ __forceinline__ void cp_async8_g(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all()
 {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
@@ -260,6 +266,124 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// refinement by zero-padded FFT (the reference's band-limited upsampling, refine.cu / cuFFT)
+// ------------------------------------------------------------------------------------------
+
+// Upsample the N x N complex tile at src (rows stride apart) by F / N and write its amplitudes
+// (F x F, dense, row stride F) to out: N-point FFTs along the rows, each row's spectrum padded
+// to F points, F-point inverses along the rows (N x F, rows upsampled); N-point FFTs down the
+// columns, then CB columns at a time: padded to F points, F-point inverses, amplitudes out.
+// Scaled by 1 / N^2.
+template <int N1, int N2, int F1, int F2>
+__device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
+                             const float2* __restrict__ twn_g, const float2* __restrict__ twf_g,
+                             float* __restrict__ out)
+{
+    constexpr int N = N1 * N2, F = F1 * F2;
+    constexpr int RSN = N + 1, RSF = F + 1, CB = 32, CBS = CB + 1;
+    constexpr int XB = (N * RSN > F * CBS ? N * RSN : F * CBS);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float2* X = reinterpret_cast<float2*>(sm);   // the tile, later a block of F-point columns
+    float2* Y = X + XB;                          // rows upsampled: N x F
+    float2* twn = Y + N * RSF;
+    float2* twf = twn + N;
+    for (int y = warp; y < N; y += kWarps)
+        for (int x = lane; x < N; x += 32) cp_async8_g(X + y * RSN + x, src + y * stride + x);
+    for (int k = tid; k < N; k += kThreads) twn[k] = __ldg(twn_g + k);
+    for (int k = tid; k < F; k += kThreads) twf[k] = __ldg(twf_g + k);
+    cp_async_wait_all();
+    __syncthreads();
+    // rows: forward N
+    for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % N) * RSN, 1, t / N, twn);
+    __syncthreads();
+    for (int t = tid; t < N * N1; t += kThreads) fft::step_b<N1, N2, -1>(X + (t % N) * RSN, 1, t / N);
+    __syncthreads();
+    // pad each row's spectrum into the F-point permutation
+    for (int y = warp; y < N; y += kWarps)
+        for (int pp = lane; pp < F; pp += 32) {
+            float w;
+            const int k = fft::pad_source<N, F>(fft::freq_at<F1, F2>(pp), w);
+            const float2 v = X[y * RSN + fft::pos_of<N1, N2>(k)];
+            Y[y * RSF + pp] = make_float2(w * v.x, w * v.y);
+        }
+    __syncthreads();
+    // rows: inverse F
+    for (int t = tid; t < N * F1; t += kThreads) fft::step_b<F1, F2, 1>(Y + (t % N) * RSF, 1, t / N);
+    __syncthreads();
+    for (int t = tid; t < N * F2; t += kThreads) fft::inv_a<F1, F2>(Y + (t % N) * RSF, 1, t / N, twf);
+    __syncthreads();
+    // columns: forward N
+    for (int t = tid; t < F * N2; t += kThreads) fft::fwd_a<N1, N2>(Y + t % F, RSF, t / F, twn);
+    __syncthreads();
+    for (int t = tid; t < F * N1; t += kThreads) fft::step_b<N1, N2, -1>(Y + t % F, RSF, t / F);
+    __syncthreads();
+    const float scale = 1.0f / ((float)N * (float)N);
+    for (int c0 = 0; c0 < F; c0 += CB) {
+        // pad a block of CB columns into the F-point permutation, inverse F, amplitudes out
+        for (int yy = warp; yy < F; yy += kWarps) {
+            float w;
+            const int k = fft::pad_source<N, F>(fft::freq_at<F1, F2>(yy), w);
+            const float2* row = Y + fft::pos_of<N1, N2>(k) * RSF + c0;
+            for (int cc = lane; cc < CB; cc += 32) {
+                const float2 v = c0 + cc < F ? row[cc] : make_float2(0.0f, 0.0f);
+                X[yy * CBS + cc] = make_float2(w * v.x, w * v.y);
+            }
+        }
+        __syncthreads();
+        for (int t = tid; t < CB * F1; t += kThreads) fft::step_b<F1, F2, 1>(X + t % CB, CBS, t / CB);
+        __syncthreads();
+        for (int t = tid; t < CB * F2; t += kThreads) fft::inv_a<F1, F2>(X + t % CB, CBS, t / CB, twf);
+        __syncthreads();
+        for (int y = warp; y < F; y += kWarps)
+            for (int cc = lane; cc < CB && c0 + cc < F; cc += 32) {
+                const float2 v = X[y * CBS + cc];
+                const float re = v.x * scale, im = v.y * scale;
+                out[(long long)y * F + c0 + cc] = sqrtf(re * re + im * im);
+            }
+        __syncthreads();
+    }
+}
+
+template <int N1, int N2, int F1, int F2>
+constexpr int fft_upsample_smem()
+{
+    constexpr int N = N1 * N2, F = F1 * F2;
+    constexpr int XB = (N * (N + 1) > F * 33 ? N * (N + 1) : F * 33);
+    return (XB + N * (F + 1) + N + F) * 8;
+}
+
+// one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window
+template <int N1, int N2, int F1, int F2>
+__global__ void __launch_bounds__(kThreads, 1)
+spec_refine_kernel(const float2* base, const long long* off, long long stride,
+                   const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
+                   const float2* twn, const float2* twf, float* refined, long long refined_stride,
+                   long long out_off)
+{
+    extern __shared__ __align__(16) unsigned char rsm[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    if (valid[p] < 0) return;
+    const float2* src = base + off[p];
+    if (coarse) {
+        const CoarseOut co = coarse[p];
+        src += co.top * stride + co.left;
+    }
+    fft_upsample<N1, N2, F1, F2>(src, stride, rsm, twn, twf,
+                                 refined + (long long)blockIdx.x * refined_stride + out_off);
+}
+
+// refinement (N, F = 2 N) pairs that are compiled: N, N1, N2, F1, F2
+#define AMPCOR_REFINE_PAIRS(X) \
+    X(16, 4, 4, 4, 8)          \
+    X(24, 4, 6, 6, 8)          \
+    X(32, 4, 8, 8, 8)          \
+    X(40, 5, 8, 8, 10)         \
+    X(48, 6, 8, 8, 12)         \
+    X(64, 8, 8, 8, 16)         \
+    X(80, 8, 10, 10, 16)
+
 // transform lengths: N, N1, N2 (N1 N2 = N)
 #define AMPCOR_SPEC_LENGTHS(X) \
     X(16, 4, 4)                \
@@ -388,10 +512,46 @@ int spec_next_length(int w)
     return 0;
 }
 
+bool spec_refine_supported(int n, int f, int& smem)
+{
+    if (f != 2) return false;
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                \
+    if (n == NN) {                                        \
+        smem = fft_upsample_smem<A, B, C, D>();           \
+        return smem <= 227 * 1024;                        \
+    }
+    AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    return false;
+}
+
+cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
+                               const long long* off, long long stride, const CoarseOut* coarse,
+                               long long pair0, long long pairs, const long long* valid,
+                               const float2* twn, const float2* twf, float* refined,
+                               long long refined_stride, long long out_off)
+{
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                     \
+    if (n == NN) {                                                                             \
+        spec_refine_kernel<A, B, C, D><<<blocks, kThreads, fft_upsample_smem<A, B, C, D>(), st>>>( \
+            base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride,  \
+            out_off);                                                                          \
+        return cudaGetLastError();                                                             \
+    }
+    AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t spec_set_smem_limits()
 {
     const int limit = 227 * 1024;
     cudaError_t e = cudaFuncSetAttribute(box_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D) \
+    if (e == cudaSuccess)                  \
+        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
 #define AMPCOR_SPEC_CASE(NN, A, B) \
     if (e == cudaSuccess)          \
         e = cudaFuncSetAttribute(spec_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);

@@ -71,6 +71,80 @@ double check2d(int W, int R, std::mt19937& g)
     return err / mag;
 }
 
+// the refinement sequence of the spectral form (rows: N-point FFT, pad, F-point inverse; then the
+// columns), against the direct FP64 Dirichlet interpolation of the same tile
+static double dirichlet(int N, double d)
+{
+    double s = 1.0;
+    if (N % 2) {
+        for (int n = 1; n <= (N - 1) / 2; ++n) s += 2.0 * cos(2.0 * M_PI * n * d / N);
+    } else {
+        for (int n = 1; n < N / 2; ++n) s += 2.0 * cos(2.0 * M_PI * n * d / N);
+        s += cos(M_PI * d);
+    }
+    return s / N;
+}
+
+template <int N1, int N2, int F1, int F2>
+double check_upsample(std::mt19937& g)
+{
+    constexpr int N = N1 * N2, F = F1 * F2, f = F / N;
+    std::normal_distribution<double> nd;
+    std::vector<float2> X(N * N), Y(N * F), C(F * F), twn(N), twf(F);
+    for (int m = 0; m < N; ++m) twn[m] = make_float2((float)cos(2 * M_PI * m / N), (float)-sin(2 * M_PI * m / N));
+    for (int m = 0; m < F; ++m) twf[m] = make_float2((float)cos(2 * M_PI * m / F), (float)-sin(2 * M_PI * m / F));
+    for (auto& v : X) v = make_float2((float)nd(g), (float)nd(g));
+    std::vector<float2> X0 = X;
+    for (int y = 0; y < N; ++y) {
+        for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(X.data() + y * N, 1, n2, twn.data());
+        for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(X.data() + y * N, 1, k1);
+        for (int pp = 0; pp < F; ++pp) {
+            float w;
+            const int k = pad_source<N, F>(freq_at<F1, F2>(pp), w);
+            const float2 v = X[y * N + pos_of<N1, N2>(k)];
+            Y[y * F + pp] = make_float2(w * v.x, w * v.y);
+        }
+        for (int k1 = 0; k1 < F1; ++k1) step_b<F1, F2, 1>(Y.data() + y * F, 1, k1);
+        for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(Y.data() + y * F, 1, n2, twf.data());
+    }
+    for (int x = 0; x < F; ++x) {
+        for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(Y.data() + x, F, n2, twn.data());
+        for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(Y.data() + x, F, k1);
+        for (int yy = 0; yy < F; ++yy) {
+            float w;
+            const int k = pad_source<N, F>(freq_at<F1, F2>(yy), w);
+            const float2 v = Y[pos_of<N1, N2>(k) * F + x];
+            C[yy * F + x] = make_float2(w * v.x, w * v.y);
+        }
+        for (int k1 = 0; k1 < F1; ++k1) step_b<F1, F2, 1>(C.data() + x, F, k1);
+        for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(C.data() + x, F, n2, twf.data());
+    }
+    // direct: out = |A X A^T|, A[i][n] = D_N(i / f - n)
+    std::vector<double> A(F * N);
+    for (int i = 0; i < F; ++i)
+        for (int n = 0; n < N; ++n) A[i * N + n] = (i % f == 0) ? (i / f == n ? 1.0 : 0.0) : dirichlet(N, (double)i / f - n);
+    double err = 0, mag = 0;
+    std::vector<double> Tr(F * N), Ti(F * N);
+    for (int i = 0; i < F; ++i)
+        for (int n = 0; n < N; ++n) {
+            double sr = 0, si = 0;
+            for (int m = 0; m < N; ++m) { sr += A[i * N + m] * X0[m * N + n].x; si += A[i * N + m] * X0[m * N + n].y; }
+            Tr[i * N + n] = sr; Ti[i * N + n] = si;
+        }
+    for (int i = 0; i < F; ++i)
+        for (int j = 0; j < F; ++j) {
+            double sr = 0, si = 0;
+            for (int n = 0; n < N; ++n) { sr += Tr[i * N + n] * A[j * N + n]; si += Ti[i * N + n] * A[j * N + n]; }
+            const double ref = hypot(sr, si);
+            const float2 v = C[i * F + j];
+            const double got = hypot((double)v.x, (double)v.y) / ((double)N * N);
+            err = fmax(err, fabs(got - ref));
+            mag = fmax(mag, ref);
+        }
+    printf("upsample %d -> %d: max |amplitude error| %.3e (max amplitude %.3f)\n", N, F, err, mag);
+    return err / mag;
+}
+
 int main()
 {
     std::mt19937 g(1);
@@ -94,6 +168,12 @@ int main()
     e2 = fmax(e2, check2d<8, 12>(90, 60, g));
     e2 = fmax(e2, check2d<6, 8>(48, 32, g));
     e2 = fmax(e2, check2d<12, 12>(144, 128, g));
-    printf("worst 1-D %.2e, worst 2-D (relative to the largest numerator) %.2e\n", e, e2);
-    return (e < 2e-6 && e2 < 5e-6) ? 0 : 1;
+    double e3 = 0;
+    e3 = fmax(e3, check_upsample<8, 8, 8, 16>(g));
+    e3 = fmax(e3, check_upsample<8, 10, 10, 16>(g));
+    e3 = fmax(e3, check_upsample<4, 8, 8, 8>(g));
+    e3 = fmax(e3, check_upsample<5, 8, 8, 10>(g));
+    printf("worst 1-D %.2e, worst 2-D (relative to the largest numerator) %.2e, worst upsampling %.2e\n",
+           e, e2, e3);
+    return (e < 2e-6 && e2 < 5e-6 && e3 < 2e-6) ? 0 : 1;
 }
