@@ -25,7 +25,7 @@ CUDA_HEADERS = ["kernels.cuh", "tile_common.cuh", "fft.cuh", "tcgen05.cuh", os.p
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC", "-shared", "-Xlinker", "--no-undefined",
 ]
 
 LIB = os.path.join(HERE, "libampcor_b200.so")

@@ -245,7 +245,8 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     return true;
 }
 
-// placement statistics kernel: column-sum slices sized so that two CTAs fit on an SM
+// placement statistics kernel: the staged window (W x (W + 1) floats) and column-sum slices of
+// SU placement rows (all of them where shared memory allows)
 bool plan_box(int R, int W, BoxGeom& g, std::string& err)
 {
     std::memset(&g, 0, sizeof(g));
@@ -255,12 +256,13 @@ bool plan_box(int R, int W, BoxGeom& g, std::string& err)
     g.VS = W + 1;
     g.nb = std::max(1, kThreads / W);
     const long row_bytes = 2L * g.VS * 8;
-    g.SU = (int)std::min<long>(g.C, (113L * 1024) / row_bytes);
+    const long win_bytes = (long)W * (W + 1) * 4;
+    g.SU = (int)std::min<long>(g.C, (227L * 1024 - win_bytes) / row_bytes);
     if (g.SU < 1) {
         err = "window too wide for the placement statistics kernel";
         return false;
     }
-    g.smem_bytes = (int)(g.SU * row_bytes);
+    g.smem_bytes = (int)(g.SU * row_bytes + win_bytes);
     return true;
 }
 
@@ -444,9 +446,14 @@ struct ampcor_handle {
     // refinement by zero-padded FFT (spectral form): twiddles of R, f R, E and f E, in that order
     bool refine_fft = false;
     float* d_tw_refine = nullptr;
-    // amplitude rasters of the spectral form (reference and secondary, one allocation)
+    // amplitude rasters of the spectral form (reference and secondary, one allocation), and the
+    // box statistics of the secondary raster (FP64 column sums, 1/sigma of every box)
     float* d_amp = nullptr;
     size_t amp_cap = 0;
+    double* d_vsum = nullptr;
+    size_t vsum_cap = 0;
+    float* d_inv_raster = nullptr;
+    size_t inv_raster_cap = 0;
     // tensor-core form
     TcGeom tcc{}, tcf{};
     NccGeom gsc{}, gsf{};
@@ -714,6 +721,25 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
     detect(src.ref_base, src.ref_count, amp_ref);
     if (!shared) detect(src.tgt_base, src.tgt_count, amp_tgt);
     CK(h, cudaGetLastError(), "launching the detection kernel");
+    // coarse box statistics once per raster where the windows tile a raster (they overlap), else
+    // per pair in the chunk loop
+    InvSource inv_c{h->d_inv_c, nullptr, 0};
+    const long long rows = src.tgt_lines - h->R + 1;
+    const bool raster_stats = src.tgt_lines > 0 && rows > 0 && src.tgt_stride <= 12288;
+    if (raster_stats) {
+        const size_t cells = (size_t)rows * (size_t)src.tgt_stride;
+        if ((rc = grow(h, h->d_vsum, h->vsum_cap, 2 * cells, "box statistics")) ||
+            (rc = grow(h, h->d_inv_raster, h->inv_raster_cap, cells, "box statistics")))
+            return rc;
+        const dim3 vg((unsigned)((src.tgt_stride + 255) / 256), (unsigned)((rows + kVBlock - 1) / kVBlock));
+        box_vsum_kernel<<<vg, 256, 0, st>>>(amp_tgt, src.tgt_lines, src.tgt_stride, h->R, h->d_vsum,
+                                            h->d_vsum + cells);
+        const int psmem = (int)((2 * (src.tgt_stride + 1) + 2 * kWarps) * sizeof(double));
+        box_inv_kernel<<<(unsigned)rows, kThreads, psmem, st>>>(h->d_vsum, h->d_vsum + cells, rows,
+                                                               src.tgt_stride, h->R, h->d_inv_raster);
+        CK(h, cudaGetLastError(), "launching the box statistics kernels");
+        inv_c = InvSource{h->d_inv_raster, src.tgt_off, src.tgt_stride};
+    }
     keep(h, 3, a0, mark(h, st));
     const SpecSource cs{amp_ref, src.ref_stride, src.ref_off, 0, amp_tgt, src.tgt_stride, src.tgt_off, 0};
     const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
@@ -721,11 +747,13 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
     for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
         cudaEvent_t a = mark(h, st);
-        box_stats_kernel<<<n, kThreads, h->bxc.smem_bytes, st>>>(cs, c0, n, src.ref_off, h->bxc, h->d_inv_c);
-        CK(h, cudaGetLastError(), "launching the coarse statistics kernel");
+        if (!raster_stats) {
+            box_stats_kernel<<<n, kThreads, h->bxc.smem_bytes, st>>>(cs, c0, n, src.ref_off, h->bxc, h->d_inv_c);
+            CK(h, cudaGetLastError(), "launching the coarse statistics kernel");
+        }
         cudaEvent_t b = mark(h, st);
         keep(h, 3, a, b);
-        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, h->d_inv_c,
+        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, inv_c,
                           reinterpret_cast<const float2*>(h->d_tw_c),
                           SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
            "launching the spectral coarse correlation");
@@ -752,7 +780,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
         CK(h, cudaGetLastError(), "launching the fine statistics kernel");
         cudaEvent_t e = mark(h, st);
         keep(h, 4, d, e);
-        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, h->d_inv_f,
+        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{h->d_inv_f, nullptr, 0},
                           reinterpret_cast<const float2*>(h->d_tw_f),
                           SpecOut{1, 0, nullptr, nullptr, h->d_fine_out, h->d_gam, refined_surfaces}),
            "launching the spectral fine correlation");
@@ -978,6 +1006,8 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_zoom_uhl);
     cudaFree(h->d_tw_refine);
     cudaFree(h->d_amp);
+    cudaFree(h->d_vsum);
+    cudaFree(h->d_inv_raster);
     cudaFree(h->d_tc_err);
     drop_marks(h);
     if (h->h_arena) cudaFreeHost(h->h_arena);
@@ -1046,7 +1076,7 @@ int ampcor_adjust(ampcor_handle* h, const float** offsets)
             (long long)P, (long long)h->R * h->R, (long long)h->W * h->W, h->d_ref_off, h->d_tgt_off);
         CK(h, cudaGetLastError(), "launching the arena offsets kernel");
         const long long cells = (long long)P * ((long long)h->R * h->R + (long long)h->W * h->W);
-        PairSource src{h->d_arena, h->d_ref_off, h->R, h->d_arena, h->d_tgt_off, h->W, cells, cells};
+        PairSource src{h->d_arena, h->d_ref_off, h->R, h->d_arena, h->d_tgt_off, h->W, cells, cells, 0};
         if ((rc = run_pipeline(h, src, (long long)P, h->d_offsets, h->d_diag, nullptr, nullptr, st))) return rc;
         CK(h, cudaMemcpyAsync(h->h_offsets, h->d_offsets, 2 * P * sizeof(float), cudaMemcpyDeviceToHost, st),
            "harvesting the offset field");
@@ -1093,7 +1123,7 @@ int ampcor_correlate(ampcor_handle* h, const ampcor_job* j, void* stream)
     CK(h, cudaGetLastError(), "launching the pair offsets kernel");
     PairSource src{static_cast<const float2*>(j->ref), h->d_ref_off, j->ref_samples,
                    static_cast<const float2*>(j->tgt), h->d_tgt_off, j->tgt_samples,
-                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples};
+                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples, j->tgt_lines};
     return run_pipeline(h, src, (long long)j->pairs, reinterpret_cast<float2*>(j->offsets),
                         reinterpret_cast<PairDiag*>(j->diag), j->coarse_surfaces,
                         j->refined_surfaces, st);
@@ -1452,7 +1482,7 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
         j->ulhc, P, j->ref_lines, j->ref_samples, j->tgt_lines, j->tgt_samples, R, W, ref_off, tgt_off, bad);
     PairSource src{static_cast<const float2*>(j->ref), ref_off, j->ref_samples,
                    static_cast<const float2*>(j->tgt), tgt_off, j->tgt_samples,
-                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples};
+                   j->ref_lines * j->ref_samples, j->tgt_lines * j->tgt_samples, j->tgt_lines};
     coarse_kernel<<<(unsigned)P, kThreads, gc.smem_bytes, st>>>(src, 0, P, gc, m, coarse, peak,
                                                                 j->coarse_surfaces);
     const int refine_smem = std::max(ic.smem_bytes, iw.smem_bytes);

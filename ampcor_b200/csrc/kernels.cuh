@@ -75,6 +75,7 @@ struct PairSource {
     long long tgt_stride;
     long long ref_count;  // samples behind ref_base (the raster or the arena)
     long long tgt_count;
+    long long tgt_lines;  // lines of the secondary raster (tgt_count / tgt_stride); 0 for the arena
 };
 
 // coarse result of one pair
@@ -212,9 +213,9 @@ struct SpecGeom {
     int smem_bytes;
 };
 
-// FP64 placement statistics of one surface per CTA (512 threads, two CTAs per SM): column sums
-// over R rows for a slice of SU placement rows at a time (nb blocks of placement rows per
-// column), then prefix sums along each row
+// FP64 placement statistics of one surface per CTA (512 threads, the window staged in shared
+// memory): column sums over R rows for a slice of SU placement rows at a time (nb blocks of
+// placement rows per column), then prefix sums along each row
 struct BoxGeom {
     int R, W, C;
     int SU;        // placement rows per slice
@@ -250,6 +251,22 @@ struct SpecOut {
 
 // |z| of every sample of a complex array (n samples)
 __global__ void detect_kernel(const float2* src, long long n, float* dst);
+// FP64 box statistics of a whole amplitude raster, for windows that overlap (the coarse stage of a
+// raster job): column sums over R rows (v1: sum a, v2: sum a^2; rows = lines - R + 1 of them),
+// then per row prefix sums and 1/sqrt(var) of the R x R box at every (y, x), x <= samples - R
+constexpr int kVBlock = 64;  // rows slid per thread of the column sums
+__global__ void box_vsum_kernel(const float* a, long long lines, long long samples, int R, double* v1,
+                                double* v2);
+__global__ void box_inv_kernel(const double* v1, const double* v2, long long rows, long long samples,
+                               int R, float* inv);
+
+// where a spectral correlation finds 1/sigma_box of placement (u, v) of chunk-local pair b:
+// base + off[pair0 + b] + u stride + v when off is given, else base + b C^2 + u C + v
+struct InvSource {
+    const float* base;
+    const long long* off;
+    long long stride;
+};
 __global__ void box_stats_kernel(SpecSource s, long long pair0, long long pairs,
                                  const long long* valid, BoxGeom g, float* inv);
 
@@ -266,7 +283,7 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
                                const float2* twn, const float2* twf, float* refined,
                                long long refined_stride, long long out_off);
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
-                        long long pair0, long long pairs, const long long* valid, const float* inv,
+                        long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out);
 
 }  // namespace ampcor_b200

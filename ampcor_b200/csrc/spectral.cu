@@ -92,7 +92,7 @@ constexpr float kSpecTol = 4e-6f;
 // Normalised surface -> first maximum (valid in every thread); optional copies of the surface.
 // The surface is built in the imaginary parts of the placement rows of the tile.
 __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const float* __restrict__ inv,
-                             float inv_sigma, double mean_c, float tnorm, const float* chip,
+                             long long is, float inv_sigma, double mean_c, float tnorm, const float* chip,
                              long long cs, const float* win, long long ws, float* out1, float* out2,
                              float& bv, int& bi)
 {
@@ -107,7 +107,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
         for (int v = lane; v < C; v += 32) {
             const int idx = u * C + v;
             float2* z = Z + u * RS + v;
-            const float inv_box = __ldg(inv + idx);
+            const float inv_box = __ldg(inv + u * is + v);
             const float gv = z->x * scale * inv_box * inv_sigma;
             z->y = gv;
             if (ebox * inv_box > kSpecTol)
@@ -124,9 +124,9 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
         float wv = -INFINITY;
         int wi = INT_MAX;
         for (int idx = warp; idx < C * C; idx += kWarps) {
-            const float inv_box = __ldg(inv + idx);
-            const float e = ebox * inv_box;
             const int u = idx / C, v = idx - u * C;
+            const float inv_box = __ldg(inv + u * is + v);
+            const float e = ebox * inv_box;
             float* gp = &Z[u * RS + v].y;
             if (!(e > kSpecTol) || !(all || *gp + e >= bv)) continue;
             float acc = 0.0f;
@@ -160,7 +160,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
 template <int N1, int N2>
 __global__ void __launch_bounds__(kThreads, 1)
 spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
-            const float* inv, const float2* tw_g, SpecOut out)
+            InvSource inv, const float2* tw_g, SpecOut out)
 {
     extern __shared__ __align__(16) unsigned char ssm[];
     if (blockIdx.x >= pairs) return;
@@ -241,10 +241,11 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 
     float bv;
     int bi;
-    const float* inv_b = inv + (long long)blockIdx.x * C * C;
+    const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
+    const long long is = inv.off ? inv.stride : C;
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
-    spec_surface(Z, red, g, inv_b, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam,
+    spec_surface(Z, red, g, inv_b, is, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam,
                  surf, bv, bi);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;
@@ -419,11 +420,129 @@ __global__ void detect_kernel(const float2* __restrict__ src, long long n, float
     }
 }
 
+__global__ void __launch_bounds__(256)
+box_vsum_kernel(const float* __restrict__ a, long long lines, long long samples, int R,
+                double* __restrict__ v1, double* __restrict__ v2)
+{
+    const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long rows = lines - R + 1;
+    const long long y0 = (long long)blockIdx.y * kVBlock;
+    if (x >= samples || y0 >= rows) return;
+    const long long y1 = y0 + kVBlock < rows ? y0 + kVBlock : rows;
+    const float* col = a + x;
+    double a1[4] = {0.0, 0.0, 0.0, 0.0}, a2[4] = {0.0, 0.0, 0.0, 0.0};
+    int i = 0;
+    for (; i + 4 <= R; i += 4) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double tv = __ldg(col + (y0 + i + k) * samples);
+            a1[k] += tv;
+            a2[k] += tv * tv;
+        }
+    }
+    for (; i < R; ++i) {
+        const double tv = __ldg(col + (y0 + i) * samples);
+        a1[0] += tv;
+        a2[0] += tv * tv;
+    }
+    double s1 = (a1[0] + a1[1]) + (a1[2] + a1[3]);
+    double s2 = (a2[0] + a2[1]) + (a2[2] + a2[3]);
+    for (long long y = y0; y < y1; ++y) {
+        v1[y * samples + x] = s1;
+        v2[y * samples + x] = s2;
+        if (y + 1 < y1) {
+            const double p = __ldg(col + (y + R) * samples), q = __ldg(col + y * samples);
+            s1 += p - q;
+            s2 += p * p - q * q;
+        }
+    }
+}
+
+// one CTA per box row: FP64 exclusive prefix sums of the row's column sums (in chunks of eight per
+// thread, a fixed order), then the box of every x from two prefix differences
+__global__ void __launch_bounds__(kThreads)
+box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, long long rows,
+               long long samples, int R, float* __restrict__ inv)
+{
+    extern __shared__ __align__(16) double psm[];
+    const long long y = blockIdx.x;
+    if (y >= rows) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P1 = psm;
+    double* P2 = psm + samples + 1;
+    double* red = P2 + samples + 1;  // 2 x kWarps
+    const double* r1 = v1 + y * samples;
+    const double* r2 = v2 + y * samples;
+    double carry1 = 0.0, carry2 = 0.0;
+    for (long long c0 = 0; c0 < samples; c0 += kThreads * 8) {
+        const long long b0 = c0 + (long long)tid * 8;
+        double l1[8], l2[8], s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const long long i = b0 + k;
+            const double p = i < samples ? __ldg(r1 + i) : 0.0;
+            const double q = i < samples ? __ldg(r2 + i) : 0.0;
+            l1[k] = s1;
+            l2[k] = s2;
+            s1 += p;
+            s2 += q;
+        }
+        // exclusive scan of the thread totals: within the warp, then across warps
+        double i1 = s1, i2 = s2;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double u1 = __shfl_up_sync(kFull, i1, o), u2 = __shfl_up_sync(kFull, i2, o);
+            if (lane >= o) {
+                i1 += u1;
+                i2 += u2;
+            }
+        }
+        if (lane == 31) {
+            red[warp] = i1;
+            red[kWarps + warp] = i2;
+        }
+        __syncthreads();
+        double w1 = 0.0, w2 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            if (w < warp) {
+                w1 += red[w];
+                w2 += red[kWarps + w];
+            }
+            t1 += red[w];
+            t2 += red[kWarps + w];
+        }
+        const double o1 = carry1 + w1 + (i1 - s1), o2 = carry2 + w2 + (i2 - s2);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const long long i = b0 + k;
+            if (i < samples) {
+                P1[i] = o1 + l1[k];
+                P2[i] = o2 + l2[k];
+            }
+        }
+        carry1 += t1;
+        carry2 += t2;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        P1[samples] = carry1;
+        P2[samples] = carry2;
+    }
+    __syncthreads();
+    const double cells = (double)R * (double)R;
+    for (long long x = tid; x + R <= samples; x += kThreads) {
+        const double b1 = P1[x + R] - P1[x];
+        const double b2 = P2[x + R] - P2[x];
+        const float var = (float)(b2 - b1 * b1 / cells);
+        inv[y * samples + x] = var > 0.0f ? __frsqrt_rn(var) : 0.0f;
+    }
+}
+
 // 1/sqrt(sum_box t^2 - (sum_box t)^2 / R^2) of every placement of a chunk-local pair (0 for a flat
 // box): the FP64 summed-area statistics of tgtStats.cu:139-162 and sat.cu:81-149, evaluated as
-// column sums slid down the window (FP64) and prefix sums along the placement rows.  The window
-// is read from L2 / HBM as it is; only the column sums live in shared memory.
-__global__ void __launch_bounds__(kThreads, 2)
+// column sums slid down the staged window (FP64, nb blocks of placement rows per column) and
+// prefix sums along the placement rows, SU placement rows per slice.
+__global__ void __launch_bounds__(kThreads, 1)
 box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long* valid, BoxGeom g,
                  float* inv)
 {
@@ -432,12 +551,17 @@ box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long
     if (valid[pair0 + blockIdx.x] < 0) return;
     const float* win = spec_win(s, pair0, blockIdx.x);
     const long long ws = s.win_stride;
-    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb;
+    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb, TS = W + 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* V1 = bsm;
     double* V2 = bsm + SU * VS;
+    float* T = reinterpret_cast<float*>(V2 + SU * VS);
     float* out = inv + (long long)blockIdx.x * C * C;
     const double cells = (double)R * (double)R;
+    for (int y = warp; y < W; y += kWarps)
+        for (int x = lane; x < W; x += 32) cp_async4(T + y * TS + x, win + y * ws + x);
+    cp_async_wait_all();
+    __syncthreads();
     for (int u0 = 0; u0 < C; u0 += SU) {
         const int nu = min(SU, C - u0);
         const int B = (nu + nb - 1) / nb;
@@ -445,19 +569,19 @@ box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long
             const int x = t % W, ub = t / W;
             const int ua = u0 + ub * B, ue = min(ua + B, u0 + nu);
             if (ua >= ue) continue;
-            const float* col = win + x;
+            const float* col = T + x;
             double a1[4] = {0.0, 0.0, 0.0, 0.0}, a2[4] = {0.0, 0.0, 0.0, 0.0};
             int i = 0;
             for (; i + 4 <= R; i += 4) {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const double tv = __ldg(col + (long long)(ua + i + k) * ws);
+                    const double tv = col[(ua + i + k) * TS];
                     a1[k] += tv;
                     a2[k] += tv * tv;
                 }
             }
             for (; i < R; ++i) {
-                const double tv = __ldg(col + (long long)(ua + i) * ws);
+                const double tv = col[(ua + i) * TS];
                 a1[0] += tv;
                 a2[0] += tv * tv;
             }
@@ -467,8 +591,7 @@ box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long
                 V1[(u - u0) * VS + x] = s1;
                 V2[(u - u0) * VS + x] = s2;
                 if (u + 1 < ue) {
-                    const double a = __ldg(col + (long long)(u + R) * ws);
-                    const double b = __ldg(col + (long long)u * ws);
+                    const double a = col[(u + R) * TS], b = col[u * TS];
                     s1 += a - b;
                     s2 += a * a - b * b;
                 }
@@ -547,6 +670,8 @@ cudaError_t spec_set_smem_limits()
 {
     const int limit = 227 * 1024;
     cudaError_t e = cudaFuncSetAttribute(box_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(box_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D) \
     if (e == cudaSuccess)                  \
         e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
@@ -561,7 +686,7 @@ cudaError_t spec_set_smem_limits()
 }
 
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
-                        long long pair0, long long pairs, const long long* valid, const float* inv,
+                        long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out)
 {
 #define AMPCOR_SPEC_CASE(NN, A, B)                                                              \
