@@ -469,6 +469,7 @@ struct ampcor_handle {
     //  4 fine statistics, 5 zoom)
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks[6];
+    uint64_t mark_kernels[6] = {0, 0, 0, 0, 0, 0};
     std::string err;
 };
 
@@ -589,9 +590,13 @@ cudaEvent_t mark(ampcor_handle* h, cudaStream_t st)
     return e;
 }
 
-void keep(ampcor_handle* h, int stage, cudaEvent_t a, cudaEvent_t b)
+// a timed stage region holding `kernels` kernel launches
+void keep(ampcor_handle* h, int stage, cudaEvent_t a, cudaEvent_t b, int kernels = 1)
 {
-    if (a && b) h->marks[stage].emplace_back(a, b);
+    if (a && b) {
+        h->marks[stage].emplace_back(a, b);
+        h->mark_kernels[stage] += (uint64_t)kernels;
+    }
 }
 
 // plain FP32 form: coarse over all pairs, then (refine -> fine) per chunk on stream st
@@ -628,6 +633,7 @@ int run_plain(ampcor_handle* h, const PairSource& src, long long pairs, float2* 
 
 void drop_marks(ampcor_handle* h)
 {
+    for (auto& k : h->mark_kernels) k = 0;
     std::vector<cudaEvent_t> seen;
     for (auto& v : h->marks) {
         for (auto& pr : v) {
@@ -740,7 +746,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
         CK(h, cudaGetLastError(), "launching the box statistics kernels");
         inv_c = InvSource{h->d_inv_raster, src.tgt_off, src.tgt_stride};
     }
-    keep(h, 3, a0, mark(h, st));
+    keep(h, 3, a0, mark(h, st), (shared ? 1 : 2) + (raster_stats ? 2 : 0));
     const SpecSource cs{amp_ref, src.ref_stride, src.ref_off, 0, amp_tgt, src.tgt_stride, src.tgt_off, 0};
     const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
@@ -752,7 +758,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
             CK(h, cudaGetLastError(), "launching the coarse statistics kernel");
         }
         cudaEvent_t b = mark(h, st);
-        keep(h, 3, a, b);
+        keep(h, 3, a, b, raster_stats ? 0 : 1);
         CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, inv_c,
                           reinterpret_cast<const float2*>(h->d_tw_c),
                           SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
@@ -775,7 +781,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
             CK(h, cudaGetLastError(), "launching the refinement kernel");
         }
         cudaEvent_t d = mark(h, st);
-        keep(h, 1, c, d);
+        keep(h, 1, c, d, h->refine_fft ? 2 : 1);
         box_stats_kernel<<<n, kThreads, h->bxf.smem_bytes, st>>>(fs, c0, n, src.ref_off, h->bxf, h->d_inv_f);
         CK(h, cudaGetLastError(), "launching the fine statistics kernel");
         cudaEvent_t e = mark(h, st);
@@ -1242,8 +1248,8 @@ int ampcor_kernel_times(ampcor_handle* h, double* ms, uint64_t* launches)
             float x = 0.0f;
             CK(h, cudaEventElapsedTime(&x, pr.first, pr.second), "reading a kernel event");
             ms[s] += x;
-            ++launches[s];
         }
+        launches[s] = h->mark_kernels[s];
     }
     drop_marks(h);
     return AMPCOR_OK;

@@ -144,14 +144,27 @@ class Server:
         return ws[key]
 
     def warm(self, jobs):
-        """Create (and exercise once) every worker the jobs will need, outside the timed loop."""
+        """Create (and exercise once) every worker the jobs will need, outside the timed loop.
+
+        Each worker runs the largest jobs of its geometry (by raster area, raster width and pair
+        count), so that the device buffers it sizes on first use (amplitude rasters, box
+        statistics, per-pair results) never grow inside the timed loop; growing one frees
+        memory, which waits for the whole device."""
         import torch
 
-        seen = set()
+        largest = {}
         for job in jobs:
-            if job.geometry in seen:
-                continue
-            seen.add(job.geometry)
+            lines, samples = job.ref.shape
+            picks = largest.setdefault(job.geometry, {})
+            for key, val in (("area", lines * samples), ("width", samples), ("pairs", job.pairs)):
+                if key not in picks or val > picks[key][0]:
+                    picks[key] = (val, job)
+        warm_jobs = []
+        for picks in largest.values():
+            for _, job in picks.values():
+                if all(job is not j for j in warm_jobs):
+                    warm_jobs.append(job)
+        for job in warm_jobs:
             for slot in range(self.slots):
                 w = self._worker(slot, job)
                 with torch.cuda.stream(self.streams[slot]):

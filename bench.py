@@ -267,6 +267,12 @@ def run_b200(args):
     ms = e0.elapsed_time(e1)
     kt = worker.kernel_times()
     launches = sum(n for _, n in kt.values())
+    # timed regions per kernel kind: one per chunk of pairs and step (the plain form's coarse
+    # kernel runs once per step over all pairs)
+    nchunks = -(-w.pairs // max(int(worker.chunk), 1))
+    kt_regions = {k: args.steps * nchunks for k in kt}
+    if worker.form == "plain":
+        kt_regions["coarse_correlation"] = args.steps
     worker.profile(False)
     clk = clocks.stop()
     # result check outside the timed region
@@ -309,42 +315,67 @@ def run_b200(args):
         Rf = w.refine_factor * w.chip
         Cf = 2 * w.refine_factor * w.refine_margin + 1
         f = w.refine_factor
-        # algorithmic flops per pair of each kernel kind (direct-form numerators; the
-        # refinement's separable interpolation)
-        flop_pair = {
-            "coarse_correlation": 2.0 * w.chip ** 2 * C ** 2,
-            "fine_correlation": 2.0 * Rf ** 2 * Cf ** 2,
-            "refinement": 4.0 * (f * f - 1) * (w.chip ** 3 + E ** 3),
-        }
+        R, W, Wf = w.chip, w.window, f * E
+        Z = w.zoom_factor * Cf
+        # algorithmic work per pair of each kernel kind: the spectral kernels are bounded by the
+        # bytes they must move (amplitude tiles in, placement statistics in, surfaces out), the
+        # direct forms by the flops of the direct-form sums, the zoom by its two products
+        if worker.form == "spectral":
+            work = {
+                "coarse_correlation": ("hbm", 4.0 * (W * W + R * R + C * C)),
+                "refinement": ("hbm", 8.0 * (R * R + E * E) + 4.0 * (Rf * Rf + Wf * Wf)),
+                "fine_statistics": ("hbm", 4.0 * (Wf * Wf + Cf * Cf)),
+                "fine_correlation": ("hbm", 4.0 * (Wf * Wf + Rf * Rf + 2 * Cf * Cf)),
+            }
+        else:
+            work = {
+                "coarse_correlation": ("tensor", 2.0 * R ** 2 * C ** 2),
+                "fine_correlation": ("tensor", 2.0 * Rf ** 2 * Cf ** 2),
+                "refinement": ("tensor", 4.0 * (f * f - 1) * (R ** 3 + E ** 3)),
+            }
+        work["zoom"] = ("tensor", 2.0 * (Z * Cf * Cf + Z * Z * Cf))
         names = {
             "coarse_correlation": {"tensor": "tc_coarse_kernel", "spectral": "spec_kernel (coarse)"}
             .get(worker.form, "coarse_kernel"),
             "fine_correlation": {"tensor": "tc_fine_kernel", "spectral": "spec_kernel (fine)"}
             .get(worker.form, "fine_kernel"),
-            "refinement": "refine_kernel",
-            "coarse_statistics": {"spectral": "detect_kernel + box_stats_kernel (coarse)"}
+            "refinement": {"spectral": "spec_refine_kernel (chip + window)"}.get(worker.form, "refine_kernel"),
+            "coarse_statistics": {"spectral": "detect_kernel + box_vsum_kernel + box_inv_kernel (per raster)"}
             .get(worker.form, "window_stats_cplx_kernel"),
             "fine_statistics": {"spectral": "box_stats_kernel (fine)"}
             .get(worker.form, "window_stats_real_kernel"),
             "zoom": "tc_zoom_kernel (zoom_kernel where Zm exceeds the tensor memory)",
         }
-        top = max(flop_pair, key=lambda k: kt[k][0])
-        top_ms, top_n = kt[top]
-        per_launch_ms = top_ms / max(top_n, 1)
-        pairs_per_launch = w.pairs * args.steps / max(top_n, 1)
-        flops = flop_pair[top] * pairs_per_launch
-        achieved = flops / (per_launch_ms / 1000.0) / 1e12
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except Exception:
             pass
-        tensor_peak = peaks.get("bf16_tflops")
-        peak_src = "of measured" if tensor_peak else "of fallback"
-        tensor_peak = tensor_peak or 1590.0
+        peak_src = "of measured" if peaks.get("bf16_tflops") else "of fallback"
+        peak_of = {"hbm": (peaks.get("hbm_gbs") or 6650.0, "GB/s", 1e9),
+                   "tensor": (peaks.get("bf16_tflops") or 1590.0, "TFLOP/s", 1e12)}
         simt = fp32_peak(local)
-        traffic = load_traffic().get(names[top])
-        traffic_per_launch = traffic["bytes_per_pair"] * pairs_per_launch if traffic else None
+        traffic_table = load_traffic()
+        kernels = {}
+        for k, (bound, per_pair) in work.items():
+            k_ms, k_n = kt.get(k, (0.0, 0))
+            if not k_n or k_ms <= 0:
+                continue
+            regions = max(kt_regions.get(k, 1), 1)
+            pairs_per_region = w.pairs * args.steps / regions
+            amount = per_pair * pairs_per_region
+            region_ms = k_ms / regions
+            peak, unit, scale = peak_of[bound]
+            if k == "zoom":
+                peak = peak / 2.0  # tf32 runs at half the bf16 rate
+            achieved = amount / (region_ms / 1000.0) / scale
+            tr = traffic_table.get(names[k])
+            kernels[k] = {"kernel": names[k], "bound": bound, "achieved": achieved, "peak": peak,
+                          "unit": unit, "frac": achieved / peak, "ms_per_step": k_ms / args.steps,
+                          "amount_per_region": amount, "ms_per_region": region_ms,
+                          "traffic": tr["bytes_per_pair"] * pairs_per_region if tr else None}
+        top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+        topk = kernels[top]
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -366,14 +397,16 @@ def run_b200(args):
                            tune=[(c["form"], c["chunk"], round(c["ms"], 3)) for c in tuned["candidates"]]
                            if tuned else None),
             "roofline": {
-                "bound": "tensor", "kernel": names[top], "achieved": achieved,
-                "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved / tensor_peak,
-                "traffic": traffic_per_launch,
-                "peak_note": (f"dense bf16 tensor peak {peak_src} (MEASURED_PEAKS.json burst); "
-                              f"achieved counts the algorithmic flops of the direct-form "
-                              f"numerator only"),
-                "fp32_simt_peak": simt, "fp32_simt_frac": achieved / simt if simt > 0 else None,
-                "algorithmic_flop_per_launch": flops, "ms_per_launch": per_launch_ms,
+                "bound": topk["bound"], "kernel": topk["kernel"], "achieved": topk["achieved"],
+                "peak": topk["peak"], "unit": topk["unit"], "frac": topk["frac"],
+                "traffic": topk["traffic"],
+                "peak_note": (f"{'HBM copy bandwidth' if topk['bound'] == 'hbm' else 'dense bf16 tensor throughput'} "
+                              f"{peak_src} (MEASURED_PEAKS.json); achieved = algorithmic "
+                              f"{'bytes' if topk['bound'] == 'hbm' else 'flops'} of one timed region "
+                              f"(one chunk of pairs) / its CUDA-event time; traffic from "
+                              f"profiles/traffic.json (ncu)"),
+                "fp32_simt_peak": simt,
+                "kernels": kernels,
                 "kernel_ms_per_step": {names[k]: v[0] / args.steps for k, v in kt.items() if v[1]},
                 "launches_per_step": {names[k]: v[1] / args.steps for k, v in kt.items() if v[1]},
             },
