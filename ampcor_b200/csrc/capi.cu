@@ -237,6 +237,8 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     off = up(off + (long)g.N * 4, 16);
     g.off_red = (int)off;
     off += 256;
+    g.off_inv = (int)off;  // the placement statistics, prefetched with the tiles
+    off = up(off + (long)g.C * g.C * 4, 16);
     if (off > 227L * 1024) {
         err = "tile geometry too large for the spectral form";
         return false;

@@ -90,9 +90,10 @@ constexpr float kSpecErr = 1e-6f;
 constexpr float kSpecTol = 4e-6f;
 
 // Normalised surface -> first maximum (valid in every thread); optional copies of the surface.
-// The surface is built in the imaginary parts of the placement rows of the tile.
-__device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const float* __restrict__ inv,
-                             long long is, float inv_sigma, double mean_c, float tnorm, const float* chip,
+// The surface is built in the imaginary parts of the placement rows of the tile; inv holds
+// 1/sigma_box of the placements in shared memory (row stride C).
+__device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const float* inv,
+                             float inv_sigma, double mean_c, float tnorm, const float* chip,
                              long long cs, const float* win, long long ws, float* out1, float* out2,
                              float& bv, int& bi)
 {
@@ -107,7 +108,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
         for (int v = lane; v < C; v += 32) {
             const int idx = u * C + v;
             float2* z = Z + u * RS + v;
-            const float inv_box = __ldg(inv + u * is + v);
+            const float inv_box = inv[idx];
             const float gv = z->x * scale * inv_box * inv_sigma;
             z->y = gv;
             if (ebox * inv_box > kSpecTol)
@@ -125,7 +126,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
         int wi = INT_MAX;
         for (int idx = warp; idx < C * C; idx += kWarps) {
             const int u = idx / C, v = idx - u * C;
-            const float inv_box = __ldg(inv + u * is + v);
+            const float inv_box = inv[idx];
             const float e = ebox * inv_box;
             float* gp = &Z[u * RS + v].y;
             if (!(e > kSpecTol) || !(all || *gp + e >= bv)) continue;
@@ -179,7 +180,10 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
     int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
     double* red = reinterpret_cast<double*>(ssm + g.off_red);
+    float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
     float* Zf = reinterpret_cast<float*>(Z);
+    const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
+    const long long is = inv.off ? inv.stride : C;
     const float* chip = spec_chip(src, pair0, blockIdx.x);
     const float* win = spec_win(src, pair0, blockIdx.x);
     const long long cs = src.chip_stride, ws = src.win_stride;
@@ -199,6 +203,9 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
                 zr[2 * x + 1] = 0.0f;
         }
     }
+    // the placement statistics land in shared memory while the transform runs
+    for (int u = warp; u < C; u += kWarps)
+        for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
     for (int k = tid; k < N; k += kThreads) {
         tw[k] = __ldg(tw_g + k);
         neg[k] = fft::neg_pos<N1, N2>(k);
@@ -206,47 +213,56 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     cp_async_wait_all();
     __syncthreads();
 
-    // chip mean (FP64) and window mean; then the zero-mean chip with 1/|r'| (refStats.cu:118-302,
-    // FP64 accumulation) and the centred window with |t'|
-    double sc = 0.0, sw = 0.0;
+    // chip mean and window mean; then the zero-mean chip with 1/|r'| (refStats.cu:118-302) and
+    // the centred window with |t'|.  Each thread sums its few dozen samples in FP32 (the chip sum
+    // compensated) and the block combines the partial sums in FP64; the chip mean is subtracted
+    // as two floats (hi + lo), so r' carries the FP64 mean.  The window mean only centres the
+    // transform's input and |t'| only scales its error bound.
+    float sc = 0.0f, cc = 0.0f, sw = 0.0f;
     for (int y = warp; y < W; y += kWarps) {
         const float2* zr = Z + y * RS;
         for (int x = lane; x < W; x += 32) {
             const float2 z = zr[x];
             sw += z.x;
-            if (y < R && x < R) sc += z.y;
+            if (y < R && x < R) {
+                const float yk = z.y - cc;
+                const float tk = sc + yk;
+                cc = (tk - sc) - yk;
+                sc = tk;
+            }
         }
     }
-    block_sum2(sc, sw, red);
-    const double mean_c = sc / ((double)R * (double)R);
-    const float mean_w = (float)(sw / ((double)W * (double)W));
-    double ss = 0.0, st = 0.0;
+    double dc = (double)sc - (double)cc, dw = sw;
+    block_sum2(dc, dw, red);
+    const double mean_c = dc / ((double)R * (double)R);
+    const float mean_w = (float)(dw / ((double)W * (double)W));
+    const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
+    float ss = 0.0f, st = 0.0f;
     for (int y = warp; y < W; y += kWarps) {
         float2* zr = Z + y * RS;
         for (int x = lane; x < W; x += 32) {
             float2 z = zr[x];
             z.x -= mean_w;
-            st += (double)z.x * (double)z.x;
+            st = fmaf(z.x, z.x, st);
             if (y < R && x < R) {
-                z.y = (float)((double)z.y - mean_c);
-                ss += (double)z.y * (double)z.y;
+                z.y = (z.y - mc_hi) - mc_lo;
+                ss = fmaf(z.y, z.y, ss);
             }
             zr[x] = z;
         }
     }
-    block_sum2(ss, st, red);
-    const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
+    double dss = ss, dst = st;
+    block_sum2(dss, dst, red);
+    const float inv_sigma = dss > 0.0 ? (float)(1.0 / sqrt(dss)) : 0.0f;
 
     fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, tid, kThreads, BlockSync{});
 
     float bv;
     int bi;
-    const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
-    const long long is = inv.off ? inv.stride : C;
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
-    spec_surface(Z, red, g, inv_b, is, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam,
-                 surf, bv, bi);
+    spec_surface(Z, red, g, invs, inv_sigma, mean_c, (float)sqrt(dst), chip, cs, win, ws, gam, surf,
+                 bv, bi);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;
         if (out.stage == 0) {
