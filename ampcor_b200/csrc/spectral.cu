@@ -370,9 +370,10 @@ constexpr int fft_upsample_smem()
     return (XB + N * (F + 1) + N + F) * 8;
 }
 
-// one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window
+// one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window; two CTAs
+// per SM where their shared memory allows
 template <int N1, int N2, int F1, int F2>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, fft_upsample_smem<N1, N2, F1, F2>() <= 113 * 1024 ? 2 : 1)
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
