@@ -247,8 +247,8 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     return true;
 }
 
-// placement statistics kernel: the staged window (W x (W + 1) floats) and column-sum slices of
-// SU placement rows (all of them where shared memory allows)
+// placement statistics kernel: a prefix scratch row per warp (FP64) and float column-sum slices
+// of SU placement rows, sized so that two CTAs fit on an SM
 bool plan_box(int R, int W, BoxGeom& g, std::string& err)
 {
     std::memset(&g, 0, sizeof(g));
@@ -257,14 +257,14 @@ bool plan_box(int R, int W, BoxGeom& g, std::string& err)
     g.C = W - R + 1;
     g.VS = W + 1;
     g.nb = std::max(1, kThreads / W);
-    const long row_bytes = 2L * g.VS * 8;
-    const long win_bytes = (long)W * (W + 1) * 4;
-    g.SU = (int)std::min<long>(g.C, (227L * 1024 - win_bytes) / row_bytes);
+    const long scratch = (long)kWarps * 2 * (W + 1) * 8;
+    const long row_bytes = 2L * g.VS * 4;
+    g.SU = (int)std::min<long>(g.C, (113L * 1024 - scratch) / row_bytes);
     if (g.SU < 1) {
         err = "window too wide for the placement statistics kernel";
         return false;
     }
-    g.smem_bytes = (int)(g.SU * row_bytes + win_bytes);
+    g.smem_bytes = (int)(scratch + g.SU * row_bytes);
     return true;
 }
 

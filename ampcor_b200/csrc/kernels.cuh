@@ -213,14 +213,14 @@ struct SpecGeom {
     int smem_bytes;
 };
 
-// FP64 placement statistics of one surface per CTA (512 threads, the window staged in shared
-// memory): column sums over R rows for a slice of SU placement rows at a time (nb blocks of
-// placement rows per column), then prefix sums along each row
+// placement statistics of one surface per CTA (512 threads, two CTAs per SM): column sums over R
+// rows for a slice of SU placement rows at a time (nb blocks of placement rows per column), then
+// FP64 prefix sums along each row
 struct BoxGeom {
     int R, W, C;
     int SU;        // placement rows per slice
     int nb;        // blocks of placement rows per column
-    int VS;        // row stride of the column-sum slices (doubles), W + 1
+    int VS;        // row stride of the column-sum slices (floats), W + 1
     int smem_bytes;
 };
 

@@ -555,11 +555,49 @@ box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, lon
     }
 }
 
+// exclusive prefix sums (FP64) of the n floats of rows a and b into Pa and Pb [0 .. n] (element n
+// the total), the two scans interleaved; one warp
+__device__ void warp_prefix2_f(const float* a, const float* b, int n, double* Pa, double* Pb)
+{
+    const int lane = threadIdx.x & 31;
+    const int per = (n + 31) / 32;
+    const int beg = min(lane * per, n), end = min(beg + per, n);
+    double la = 0.0, lb = 0.0;
+    for (int k = beg; k < end; ++k) {
+        la += (double)a[k];
+        lb += (double)b[k];
+    }
+    double ia = la, ib = lb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double ya = __shfl_up_sync(kFull, ia, o);
+        const double yb = __shfl_up_sync(kFull, ib, o);
+        if (lane >= o) {
+            ia += ya;
+            ib += yb;
+        }
+    }
+    double ra = ia - la, rb = ib - lb;
+    for (int k = beg; k < end; ++k) {
+        Pa[k] = ra;
+        Pb[k] = rb;
+        ra += (double)a[k];
+        rb += (double)b[k];
+    }
+    if (end == n && beg < n) {
+        Pa[n] = ra;
+        Pb[n] = rb;
+    }
+    __syncwarp();
+}
+
 // 1/sqrt(sum_box t^2 - (sum_box t)^2 / R^2) of every placement of a chunk-local pair (0 for a flat
-// box): the FP64 summed-area statistics of tgtStats.cu:139-162 and sat.cu:81-149, evaluated as
-// column sums slid down the staged window (FP64, nb blocks of placement rows per column) and
-// prefix sums along the placement rows, SU placement rows per slice.
-__global__ void __launch_bounds__(kThreads, 1)
+// box): the summed-area statistics of tgtStats.cu:139-162 and sat.cu:81-149.  Column sums over R
+// rows (compensated FP32 for the first box of a block of placement rows, then slid down in FP64,
+// nb blocks per column) straight from the window in L2 / HBM, kept as floats for SU placement
+// rows at a time; then FP64 prefix sums along each placement row (a warp per row, its own
+// scratch) and the box of every placement from two prefix differences.  Two CTAs per SM.
+__global__ void __launch_bounds__(kThreads, 2)
 box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long* valid, BoxGeom g,
                  float* inv)
 {
@@ -568,17 +606,15 @@ box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long
     if (valid[pair0 + blockIdx.x] < 0) return;
     const float* win = spec_win(s, pair0, blockIdx.x);
     const long long ws = s.win_stride;
-    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb, TS = W + 1;
+    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* V1 = bsm;
-    double* V2 = bsm + SU * VS;
-    float* T = reinterpret_cast<float*>(V2 + SU * VS);
+    double* P1 = bsm + warp * 2 * (W + 1);  // this warp's prefix scratch
+    double* P2 = P1 + (W + 1);
+    float* V1 = reinterpret_cast<float*>(bsm + kWarps * 2 * (W + 1));
+    float* V2 = V1 + SU * VS;
     float* out = inv + (long long)blockIdx.x * C * C;
-    const double cells = (double)R * (double)R;
-    for (int y = warp; y < W; y += kWarps)
-        for (int x = lane; x < W; x += 32) cp_async4(T + y * TS + x, win + y * ws + x);
-    cp_async_wait_all();
-    __syncthreads();
+    const double rcells = 1.0 / ((double)R * (double)R);
+    constexpr int kBatch = 8;  // window rows loaded before they are summed
     for (int u0 = 0; u0 < C; u0 += SU) {
         const int nu = min(SU, C - u0);
         const int B = (nu + nb - 1) / nb;
@@ -586,45 +622,46 @@ box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long
             const int x = t % W, ub = t / W;
             const int ua = u0 + ub * B, ue = min(ua + B, u0 + nu);
             if (ua >= ue) continue;
-            const float* col = T + x;
-            double a1[4] = {0.0, 0.0, 0.0, 0.0}, a2[4] = {0.0, 0.0, 0.0, 0.0};
-            int i = 0;
-            for (; i + 4 <= R; i += 4) {
+            const float* col = win + x + (long long)ua * ws;
+            float s1 = 0.0f, c1 = 0.0f, s2 = 0.0f, c2 = 0.0f;
+            for (int i0 = 0; i0 < R; i0 += kBatch) {
+                float tb[kBatch];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const double tv = col[(ua + i + k) * TS];
-                    a1[k] += tv;
-                    a2[k] += tv * tv;
+                for (int k = 0; k < kBatch; ++k) tb[k] = i0 + k < R ? __ldg(col + (long long)(i0 + k) * ws) : 0.0f;
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) {
+                    const float tv = tb[k];
+                    const float y1 = tv - c1, t1 = s1 + y1;
+                    c1 = (t1 - s1) - y1;
+                    s1 = t1;
+                    const float y2 = tv * tv - c2, t2 = s2 + y2;
+                    c2 = (t2 - s2) - y2;
+                    s2 = t2;
                 }
             }
-            for (; i < R; ++i) {
-                const double tv = col[(ua + i) * TS];
-                a1[0] += tv;
-                a2[0] += tv * tv;
-            }
-            double s1 = (a1[0] + a1[1]) + (a1[2] + a1[3]);
-            double s2 = (a2[0] + a2[1]) + (a2[2] + a2[3]);
+            col = win + x;
+            double d1 = (double)s1 - (double)c1, d2 = (double)s2 - (double)c2;
             for (int u = ua; u < ue; ++u) {
-                V1[(u - u0) * VS + x] = s1;
-                V2[(u - u0) * VS + x] = s2;
+                V1[(u - u0) * VS + x] = (float)d1;
+                V2[(u - u0) * VS + x] = (float)d2;
                 if (u + 1 < ue) {
-                    const double a = col[(u + R) * TS], b = col[u * TS];
-                    s1 += a - b;
-                    s2 += a * a - b * b;
+                    const double a = __ldg(col + (long long)(u + R) * ws);
+                    const double b = __ldg(col + (long long)u * ws);
+                    d1 += a - b;
+                    d2 += a * a - b * b;
                 }
             }
         }
         __syncthreads();
         for (int r = warp; r < nu; r += kWarps) {
-            warp_prefix(V1 + r * VS, W);
-            warp_prefix(V2 + r * VS, W);
-            __syncwarp();
+            warp_prefix2_f(V1 + r * VS, V2 + r * VS, W, P1, P2);
             for (int v = lane; v < C; v += 32) {
-                const double b1 = V1[r * VS + v + R] - V1[r * VS + v];
-                const double b2 = V2[r * VS + v + R] - V2[r * VS + v];
-                const float var = (float)(b2 - b1 * b1 / cells);
+                const double b1 = P1[v + R] - P1[v];
+                const double b2 = P2[v + R] - P2[v];
+                const float var = (float)(b2 - b1 * b1 * rcells);
                 out[(u0 + r) * C + v] = var > 0.0f ? __frsqrt_rn(var) : 0.0f;
             }
+            __syncwarp();
         }
         __syncthreads();
     }
