@@ -287,11 +287,10 @@ bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
     const int full = g.Z / 128, rem = g.Z - 128 * full;
     g.mtiles = full + (rem ? 1 : 0);
     g.last_m = (rem == 0 || rem > 64) ? 128 : 64;
-    // accumulators: Zm parts at columns 0 and 256; the tiles of T^T at columns 64 mt
-    const int cols = std::max(g.nparts == 2 ? 512 : g.npart, 64 * g.mtiles);
-    g.tmem_cols = 32;
-    while (g.tmem_cols < cols) g.tmem_cols *= 2;
-    if (g.tmem_cols > 512) return false;
+    // accumulators: two buffers of one Zm unit (npart columns) at columns 0 and 256; the row
+    // tiles of T^T at columns 64 mt
+    g.tmem_cols = 512;
+    if (64 * g.mtiles > 512) return false;
     const long rg = (long)g.KC * 128;
     const long plane_a = (long)((g.Z + 7) / 8) * rg;
     const long plane_b = (long)(g.nparts * g.npart / 8) * rg;
@@ -309,7 +308,7 @@ bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
     g.off_glo = (int)(off += plane_g);
     off += plane_g;
     g.off_bar = (int)off;
-    off += 16;
+    off += 32;  // four mbarriers
     g.off_misc = (int)off;
     off += 128;
     g.smem_bytes = (int)off;

@@ -56,8 +56,9 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
     float* blo = reinterpret_cast<float*>(zsm + zt.off_blo);
     float* ghi = reinterpret_cast<float*>(zsm + zt.off_ghi);
     float* glo = reinterpret_cast<float*>(zsm + zt.off_glo);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(zsm + zt.off_bar);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(zsm + zt.off_bar);  // the first product
     uint64_t* drain = bar + 1;
+    uint64_t* ubar = bar + 2;  // the two accumulator buffers of Zm
     unsigned char* misc = zsm + zt.off_misc;
     uint32_t* tmem_s = reinterpret_cast<uint32_t*>(misc);
     volatile int* err = reinterpret_cast<volatile int*>(misc + 8);
@@ -73,6 +74,8 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         *err = 0;
         mbar_init(bar, 1);
         mbar_init(drain, 1);
+        mbar_init(ubar, 1);
+        mbar_init(ubar + 1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -86,9 +89,9 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
     const uint32_t ahi_a = saddr(ahi), alo_a = saddr(zsm + zt.off_alo);
     const uint32_t bhi_a = saddr(bhi), blo_a = saddr(blo), ghi_a = saddr(ghi), glo_a = saddr(glo);
     const uint32_t rg_bytes = (uint32_t)KC * 128u;  // one 8-row group of a plane
-    const int bq = zt.nparts * zt.npart;            // rows of the B planes
-    const int nchunks = bq / 16;                    // 16-column accumulator chunks of a Zm tile
-    uint32_t phase = 0;
+    const int units = zt.mtiles * zt.nparts;        // (row tile, column part) units of Zm
+    const int pch = zt.npart / 16;                  // 16-column accumulator chunks of a unit
+    uint32_t phase = 0, uph0 = 0, uph1 = 0;
     bool issued = false;
 
     // A x B -> tensor memory at column d: K steps of 8 (two 16-byte chunks), three products each
@@ -188,48 +191,54 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         __syncthreads();
         tc_fence_after();
 
-        // Zm = U T, one row tile at a time (its parts at accumulator columns 0 and 256)
+        // Zm = U T, one (row tile, column part) unit at a time, double-buffered in tensor memory
+        // (columns 0 and 256): the MMAs of the next unit run while the warps read this one
+        auto issue_unit = [&](int un) {
+            const int mt = un / zt.nparts, np = un - mt * zt.nparts;
+            const int M = (mt == zt.mtiles - 1) ? zt.last_m : 128;
+            const uint32_t arow = (uint32_t)(mt * 16) * rg_bytes;
+            const uint32_t brow = (uint32_t)(np * zt.npart / 8) * rg_bytes;
+            issue(tmem + (uint32_t)((un & 1) * 256), ahi_a + arow, alo_a + arow, bhi_a + brow,
+                  blo_a + brow, instr_desc_tf32(M, zt.npart));
+            mma_commit(ubar + (un & 1));
+        };
         float bv = -INFINITY;
         int bi = INT_MAX;
-        for (int mt = 0; mt < zt.mtiles; ++mt) {
+        if (tid == 0 && units > 0 && !*err) issue_unit(0);
+        for (int un = 0; un < units; ++un) {
             if (*err) break;
-            const int M = (mt == zt.mtiles - 1) ? zt.last_m : 128;
-            if (tid == 0) {
-                const uint32_t arow = (uint32_t)(mt * 16) * rg_bytes;
-                for (int np = 0; np < zt.nparts; ++np) {
-                    const uint32_t brow = (uint32_t)(np * zt.npart / 8) * rg_bytes;
-                    issue(tmem + (uint32_t)(np * 256), ahi_a + arow, alo_a + arow, bhi_a + brow,
-                          blo_a + brow, instr_desc_tf32(M, zt.npart));
-                }
-                mma_commit(bar);
-            }
+            if (tid == 0 && un + 1 < units) issue_unit(un + 1);
             __syncwarp();
-            const bool ok = wait_mma();
+            const bool odd = (un & 1) != 0;
+            const bool ok = mbar_wait(ubar + (un & 1), odd ? uph1 : uph0, err);
+            if (odd)
+                uph1 ^= 1u;
+            else
+                uph0 ^= 1u;
+            tc_fence_after();
+            const int mt = un / zt.nparts, np = un - mt * zt.nparts;
+            const int M = (mt == zt.mtiles - 1) ? zt.last_m : 128;
             const int row = tile_row(M, quarter, lane);
             const int pz = mt * 128 + row;
             const bool live = ok && row >= 0 && pz < Z;
+            const uint32_t dbase = tmem + lane_base(quarter) + (uint32_t)((un & 1) * 256);
             // 16-column chunks alternate between the warp groups, kZBatch loads in flight; a
-            // thread visits its columns in increasing order, so a strict comparison keeps the
-            // first maximum
-            for (int c = group; c < nchunks; c += 2 * kZBatch) {
+            // thread visits its columns in increasing order (parts in order, chunks in order), so
+            // a strict comparison keeps the first maximum
+            for (int c = group; c < pch; c += 2 * kZBatch) {
                 uint32_t r[kZBatch][16];
 #pragma unroll
-                for (int j = 0; j < kZBatch; ++j) {
-                    const int ci = c + 2 * j;
-                    if (ci < nchunks) {
-                        const int q0 = 16 * ci, np = q0 / zt.npart;
-                        tmem_ld16_async(tmem + lane_base(quarter) + (uint32_t)(np * 256 + q0 - np * zt.npart), r[j]);
-                    }
-                }
+                for (int j = 0; j < kZBatch; ++j)
+                    if (c + 2 * j < pch) tmem_ld16_async(dbase + (uint32_t)(16 * (c + 2 * j)), r[j]);
 #pragma unroll
                 for (int j = 0; j < kZBatch; ++j)
-                    if (c + 2 * j < nchunks) tmem_wait_ld(r[j]);
+                    if (c + 2 * j < pch) tmem_wait_ld(r[j]);
                 if (!live) continue;
 #pragma unroll
                 for (int j = 0; j < kZBatch; ++j) {
                     const int ci = c + 2 * j;
-                    if (ci >= nchunks) break;
-                    const int q0 = 16 * ci;
+                    if (ci >= pch) break;
+                    const int q0 = np * zt.npart + 16 * ci;
                     float v[16];
 #pragma unroll
                     for (int k = 0; k < 16; ++k) v[k] = q0 + k < Z ? __uint_as_float(r[j][k]) : -INFINITY;
