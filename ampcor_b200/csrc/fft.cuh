@@ -260,6 +260,35 @@ HD void fwd_a(float2* base, int es, int n2, const float2* tw)
     for (int k1 = 0; k1 < N1; ++k1) base[(N2 * k1 + n2) * es] = a[k1];
 }
 
+// Centring applied on the way in (the first pass over the rows): element n of row y gets sx
+// taken off its real part when y < wx and n < wx, and syh then syl off its imaginary part when
+// y < wy and n < wy.  Zero shifts leave the tile as it is.
+struct Centre {
+    float sx;
+    int wx;
+    float syh, syl;
+    int wy;
+};
+
+template <int N1, int N2>
+HD void fwd_a_centred(float2* row, int y, int n2, const float2* tw, const Centre& c)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        const int n = N2 * n1 + n2;
+        float2 v = row[n];
+        if (y < c.wx && n < c.wx) v.x -= c.sx;
+        if (y < c.wy && n < c.wy) v.y = (v.y - c.syh) - c.syl;
+        a[n1] = v;
+    }
+    Dft<N1, -1>::run(a);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[n2 * k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) row[N2 * k1 + n2] = a[k1];
+}
+
 template <int N1, int N2, int S>
 HD void step_b(float2* base, int es, int k1)
 {
@@ -332,20 +361,21 @@ HD int pad_source(int kp, float& w)
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)
 // holding t + i r: the window t in the real parts, the chip r in the imaginary parts, zero
-// outside them.  Rows at and past rows_in are all zero.  neg[p] = neg_pos(p) for p < N.
+// outside them, centred on the way in as `centre` says.  Rows at and past rows_in are all zero.
+// neg[p] = neg_pos(p) for p < N.
 // Afterwards, for u < rows_out and v < N, Z[u][v].x holds 4 N^2 sum_ij r(i, j) t(u + i, v + j)
 // (circular indices, which never wrap for the placements of a window of at most N samples).  The
 // tasks of each phase are spread over the nt threads; sync() separates the phases
 // (__syncthreads on the device).
 template <int N1, int N2, class Sync>
 HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
-                       const int* neg, int tid, int nt, Sync sync)
+                       const int* neg, const Centre& centre, int tid, int nt, Sync sync)
 {
     constexpr int N = N1 * N2;
-    // forward along rows: lanes take consecutive rows
+    // forward along rows (centring the tile on the way in): lanes take consecutive rows
     for (int t = tid; t < rows_in * N2; t += nt) {
         const int y = t % rows_in, n2 = t / rows_in;
-        fwd_a<N1, N2>(Z + y * RS, 1, n2, tw);
+        fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre);
     }
     sync();
     for (int t = tid; t < rows_in * N1; t += nt) {

@@ -213,55 +213,54 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     cp_async_wait_all();
     __syncthreads();
 
-    // chip mean and window mean; then the zero-mean chip with 1/|r'| (refStats.cu:118-302) and
-    // the centred window with |t'|.  Each thread sums its few dozen samples in FP32 (the chip sum
-    // compensated) and the block combines the partial sums in FP64; the chip mean is subtracted
-    // as two floats (hi + lo), so r' carries the FP64 mean.  The window mean only centres the
-    // transform's input and |t'| only scales its error bound.
-    float sc = 0.0f, cc = 0.0f, sw = 0.0f;
-    for (int y = warp; y < W; y += kWarps) {
-        const float2* zr = Z + y * RS;
-        for (int x = lane; x < W; x += 32) {
-            const float2 z = zr[x];
-            sw += z.x;
-            if (y < R && x < R) {
-                const float yk = z.y - cc;
-                const float tk = sc + yk;
-                cc = (tk - sc) - yk;
-                sc = tk;
+    // One sweep of sums, combined across the block in FP64: the window's sum and sum of squares,
+    // the chip's sum (compensated) and sum of squares, each thread over a few dozen samples in
+    // FP32.  They give the chip mean, 1/|r'| with |r'|^2 = sum r^2 - R^2 mean^2 (refStats.cu:118-302)
+    // and |t'| of the centred window; the centring itself (window mean off the real parts, chip
+    // mean off the imaginary parts, the latter as two floats so that r' carries the FP64 mean)
+    // happens as the first transform pass reads the tile.  The window mean only conditions the
+    // transform and |t'| only scales its error bound.
+    double acc4[4];
+    {
+        float sw = 0.0f, sw2 = 0.0f, sc = 0.0f, cc = 0.0f, sc2 = 0.0f;
+        for (int y = warp; y < W; y += kWarps) {
+            const float2* zr = Z + y * RS;
+            for (int x = lane; x < W; x += 32) {
+                const float2 z = zr[x];
+                sw += z.x;
+                sw2 = fmaf(z.x, z.x, sw2);
+                if (y < R && x < R) {
+                    const float yk = z.y - cc;
+                    const float tk = sc + yk;
+                    cc = (tk - sc) - yk;
+                    sc = tk;
+                    sc2 = fmaf(z.y, z.y, sc2);
+                }
             }
         }
+        acc4[0] = (double)sc - (double)cc;
+        acc4[1] = sc2;
+        acc4[2] = sw;
+        acc4[3] = sw2;
+        block_sum2(acc4[0], acc4[1], red);
+        block_sum2(acc4[2], acc4[3], red);
     }
-    double dc = (double)sc - (double)cc, dw = sw;
-    block_sum2(dc, dw, red);
-    const double mean_c = dc / ((double)R * (double)R);
-    const float mean_w = (float)(dw / ((double)W * (double)W));
+    const double cells_c = (double)R * (double)R, cells_w = (double)W * (double)W;
+    const double mean_c = acc4[0] / cells_c;
+    const double ss = acc4[1] - cells_c * mean_c * mean_c;
+    const double mean_w = acc4[2] / cells_w;
+    const double st = fmax(acc4[3] - cells_w * mean_w * mean_w, 0.0);
+    const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
     const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
-    float ss = 0.0f, st = 0.0f;
-    for (int y = warp; y < W; y += kWarps) {
-        float2* zr = Z + y * RS;
-        for (int x = lane; x < W; x += 32) {
-            float2 z = zr[x];
-            z.x -= mean_w;
-            st = fmaf(z.x, z.x, st);
-            if (y < R && x < R) {
-                z.y = (z.y - mc_hi) - mc_lo;
-                ss = fmaf(z.y, z.y, ss);
-            }
-            zr[x] = z;
-        }
-    }
-    double dss = ss, dst = st;
-    block_sum2(dss, dst, red);
-    const float inv_sigma = dss > 0.0 ? (float)(1.0 / sqrt(dss)) : 0.0f;
+    const fft::Centre centre{(float)mean_w, W, mc_hi, mc_lo, R};
 
-    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, tid, kThreads, BlockSync{});
+    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, centre, tid, kThreads, BlockSync{});
 
     float bv;
     int bi;
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
-    spec_surface(Z, red, g, invs, inv_sigma, mean_c, (float)sqrt(dst), chip, cs, win, ws, gam, surf,
+    spec_surface(Z, red, g, invs, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam, surf,
                  bv, bi);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;

@@ -41,33 +41,47 @@ double check1d(std::mt19937& g)
 }
 
 template <int N1, int N2>
-double check2d(int W, int R, std::mt19937& g)
+double check2d(int W, int R, std::mt19937& g, bool centre_in_pass = false)
 {
     constexpr int N = N1 * N2;
     const int C = W - R + 1, RS = N + 1;
     std::uniform_real_distribution<double> ud(0.0, 2.0);
-    std::vector<float> t(W * W), r(R * R);
+    std::vector<float> t(W * W), r(R * R), raw(R * R);
     for (auto& v : t) v = (float)ud(g);
     double mr = 0;
-    for (auto& v : r) { v = (float)ud(g); mr += v; }
+    for (auto& v : raw) { v = (float)ud(g); mr += v; }
     mr /= R * R;
-    for (auto& v : r) v = (float)(v - mr);
+    for (int k = 0; k < R * R; ++k) r[k] = (float)(raw[k] - mr);
     std::vector<float2> Z(N * RS, make_float2(0, 0)), tw(N);
     for (int m = 0; m < N; ++m) tw[m] = make_float2((float)cos(2 * M_PI * m / N), (float)-sin(2 * M_PI * m / N));
+    // with centre_in_pass the tile takes the raw chip and the window, and the first transform pass
+    // takes both means off
+    double mw = 0;
+    for (auto v : t) mw += v;
+    mw /= (double)W * W;
     for (int y = 0; y < W; ++y) for (int x = 0; x < W; ++x) Z[y * RS + x].x = t[y * W + x];
-    for (int y = 0; y < R; ++y) for (int x = 0; x < R; ++x) Z[y * RS + x].y = r[y * R + x];
+    for (int y = 0; y < R; ++y)
+        for (int x = 0; x < R; ++x) Z[y * RS + x].y = centre_in_pass ? raw[y * R + x] : r[y * R + x];
+    Centre ctr{0.0f, 0, 0.0f, 0.0f, 0};
+    if (centre_in_pass) {
+        const float hi = (float)mr;
+        ctr = Centre{(float)mw, W, hi, (float)(mr - (double)hi), R};
+    }
     std::vector<int> neg(N);
     for (int q = 0; q < N; ++q) neg[q] = neg_pos<N1, N2>(q);
-    correlate_tile<N1, N2>(Z.data(), RS, W, C, tw.data(), neg.data(), 0, 1, NoSync{});
+    correlate_tile<N1, N2>(Z.data(), RS, W, C, tw.data(), neg.data(), ctr, 0, 1, NoSync{});
     double err = 0, mag = 0;
     for (int u = 0; u < C; ++u) for (int v = 0; v < C; ++v) {
         double s = 0;
-        for (int i = 0; i < R; ++i) for (int j = 0; j < R; ++j) s += (double)r[i * R + j] * t[(u + i) * W + v + j];
+        for (int i = 0; i < R; ++i)
+            for (int j = 0; j < R; ++j)
+                s += (centre_in_pass ? (double)raw[i * R + j] - mr : (double)r[i * R + j]) * t[(u + i) * W + v + j];
         const double f = Z[u * RS + v].x / (4.0 * N * N);
         err = fmax(err, fabs(f - s));
         mag = fmax(mag, fabs(s));
     }
-    printf("2-D N=%d W=%d R=%d C=%d: max err %.3e, max |num| %.3e\n", N, W, R, C, err, mag);
+    printf("2-D N=%d W=%d R=%d C=%d%s: max err %.3e, max |num| %.3e\n", N, W, R, C,
+           centre_in_pass ? " (centred in the first pass)" : "", err, mag);
     return err / mag;
 }
 
@@ -168,6 +182,9 @@ int main()
     e2 = fmax(e2, check2d<8, 12>(90, 60, g));
     e2 = fmax(e2, check2d<6, 8>(48, 32, g));
     e2 = fmax(e2, check2d<12, 12>(144, 128, g));
+    e2 = fmax(e2, check2d<8, 16>(128, 64, g, true));
+    e2 = fmax(e2, check2d<10, 16>(160, 128, g, true));
+    e2 = fmax(e2, check2d<8, 12>(90, 60, g, true));
     double e3 = 0;
     e3 = fmax(e3, check_upsample<8, 8, 8, 16>(g));
     e3 = fmax(e3, check_upsample<8, 10, 10, 16>(g));
