@@ -357,6 +357,27 @@ HD int pad_source(int kp, float& w)
     return 0;
 }
 
+// The first inverse step (step B) of an F-point transform whose input is an N-point spectrum
+// padded to F points (pad_source): the task of k1 gathers its F2 inputs straight from the
+// N-point spectrum at src (element stride src_es, in the N-point permutation), weighted, and
+// writes the step's outputs to dst (element stride dst_es).  src and dst must not overlap.
+template <int N1, int N2, int F1, int F2>
+HD void step_b_pad(const float2* src, int src_es, float2* dst, int dst_es, int k1)
+{
+    constexpr int N = N1 * N2, F = F1 * F2;
+    float2 a[F2];
+#pragma unroll
+    for (int j = 0; j < F2; ++j) {
+        float w;
+        const int k = pad_source<N, F>(k1 + F1 * j, w);
+        const float2 v = src[pos_of<N1, N2>(k) * src_es];
+        a[j] = make_float2(w * v.x, w * v.y);
+    }
+    Dft<F2, 1>::run(a);
+#pragma unroll
+    for (int j = 0; j < F2; ++j) dst[(F2 * k1 + j) * dst_es] = a[j];
+}
+
 // ---- the 2-D correlation of one tile pair -------------------------------------------------
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)

@@ -287,17 +287,17 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 // ------------------------------------------------------------------------------------------
 
 // Upsample the N x N complex tile at src (rows stride apart) by F / N and write its amplitudes
-// (F x F, dense, row stride F) to out: N-point FFTs along the rows, each row's spectrum padded
-// to F points, F-point inverses along the rows (N x F, rows upsampled); N-point FFTs down the
-// columns, then CB columns at a time: padded to F points, F-point inverses, amplitudes out.
-// Scaled by 1 / N^2.
-template <int N1, int N2, int F1, int F2>
+// (F x F, dense, row stride F) to out: N-point FFTs along the rows; F-point inverses along the
+// rows whose first step reads the N-point spectra padded on the fly (N x F, rows upsampled);
+// N-point FFTs down the columns; then CB columns at a time the F-point inverses, again padding on
+// the fly, and the amplitudes out.  Scaled by 1 / N^2.
+template <int N1, int N2, int F1, int F2, int CB>
 __device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
                              const float2* __restrict__ twn_g, const float2* __restrict__ twf_g,
                              float* __restrict__ out)
 {
     constexpr int N = N1 * N2, F = F1 * F2;
-    constexpr int RSN = N + 1, RSF = F + 1, CB = 32, CBS = CB + 1;
+    constexpr int RSN = N + 1, RSF = F + 1, CBS = CB + 1;
     constexpr int XB = (N * RSN > F * CBS ? N * RSN : F * CBS);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float2* X = reinterpret_cast<float2*>(sm);   // the tile, later a block of F-point columns
@@ -315,17 +315,9 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     __syncthreads();
     for (int t = tid; t < N * N1; t += kThreads) fft::step_b<N1, N2, -1>(X + (t % N) * RSN, 1, t / N);
     __syncthreads();
-    // pad each row's spectrum into the F-point permutation
-    for (int y = warp; y < N; y += kWarps)
-        for (int pp = lane; pp < F; pp += 32) {
-            float w;
-            const int k = fft::pad_source<N, F>(fft::freq_at<F1, F2>(pp), w);
-            const float2 v = X[y * RSN + fft::pos_of<N1, N2>(k)];
-            Y[y * RSF + pp] = make_float2(w * v.x, w * v.y);
-        }
-    __syncthreads();
-    // rows: inverse F
-    for (int t = tid; t < N * F1; t += kThreads) fft::step_b<F1, F2, 1>(Y + (t % N) * RSF, 1, t / N);
+    // rows: inverse F, the first step padding each row's spectrum as it reads it
+    for (int t = tid; t < N * F1; t += kThreads)
+        fft::step_b_pad<N1, N2, F1, F2>(X + (t % N) * RSN, 1, Y + (t % N) * RSF, 1, t / N);
     __syncthreads();
     for (int t = tid; t < N * F2; t += kThreads) fft::inv_a<F1, F2>(Y + (t % N) * RSF, 1, t / N, twf);
     __syncthreads();
@@ -336,23 +328,20 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     __syncthreads();
     const float scale = 1.0f / ((float)N * (float)N);
     for (int c0 = 0; c0 < F; c0 += CB) {
-        // pad a block of CB columns into the F-point permutation, inverse F, amplitudes out
-        for (int yy = warp; yy < F; yy += kWarps) {
-            float w;
-            const int k = fft::pad_source<N, F>(fft::freq_at<F1, F2>(yy), w);
-            const float2* row = Y + fft::pos_of<N1, N2>(k) * RSF + c0;
-            for (int cc = lane; cc < CB; cc += 32) {
-                const float2 v = c0 + cc < F ? row[cc] : make_float2(0.0f, 0.0f);
-                X[yy * CBS + cc] = make_float2(w * v.x, w * v.y);
-            }
+        const int nc = F - c0 < CB ? F - c0 : CB;
+        // a block of columns: inverse F (padding on the fly), amplitudes out
+        for (int t = tid; t < CB * F1; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) fft::step_b_pad<N1, N2, F1, F2>(Y + c0 + cc, RSF, X + cc, CBS, t / CB);
         }
         __syncthreads();
-        for (int t = tid; t < CB * F1; t += kThreads) fft::step_b<F1, F2, 1>(X + t % CB, CBS, t / CB);
-        __syncthreads();
-        for (int t = tid; t < CB * F2; t += kThreads) fft::inv_a<F1, F2>(X + t % CB, CBS, t / CB, twf);
+        for (int t = tid; t < CB * F2; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) fft::inv_a<F1, F2>(X + cc, CBS, t / CB, twf);
+        }
         __syncthreads();
         for (int y = warp; y < F; y += kWarps)
-            for (int cc = lane; cc < CB && c0 + cc < F; cc += 32) {
+            for (int cc = lane; cc < nc; cc += 32) {
                 const float2 v = X[y * CBS + cc];
                 const float re = v.x * scale, im = v.y * scale;
                 out[(long long)y * F + c0 + cc] = sqrtf(re * re + im * im);
@@ -361,18 +350,21 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     }
 }
 
+// shared memory of the upsampling and its column block: 64 columns where the tile needs a whole
+// SM anyway, else 32 (two CTAs per SM fit)
 template <int N1, int N2, int F1, int F2>
-constexpr int fft_upsample_smem()
-{
-    constexpr int N = N1 * N2, F = F1 * F2;
-    constexpr int XB = (N * (N + 1) > F * 33 ? N * (N + 1) : F * 33);
-    return (XB + N * (F + 1) + N + F) * 8;
-}
+struct UpsampleGeom {
+    static constexpr int N = N1 * N2, F = F1 * F2;
+    static constexpr int smem32 = ((N * (N + 1) > F * 33 ? N * (N + 1) : F * 33) + N * (F + 1) + N + F) * 8;
+    static constexpr int CB = smem32 <= 113 * 1024 ? 32 : 64;
+    static constexpr int smem =
+        ((N * (N + 1) > F * (CB + 1) ? N * (N + 1) : F * (CB + 1)) + N * (F + 1) + N + F) * 8;
+};
 
 // one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window; two CTAs
 // per SM where their shared memory allows
 template <int N1, int N2, int F1, int F2>
-__global__ void __launch_bounds__(kThreads, fft_upsample_smem<N1, N2, F1, F2>() <= 113 * 1024 ? 2 : 1)
+__global__ void __launch_bounds__(kThreads, UpsampleGeom<N1, N2, F1, F2>::smem <= 113 * 1024 ? 2 : 1)
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
@@ -387,8 +379,8 @@ spec_refine_kernel(const float2* base, const long long* off, long long stride,
         const CoarseOut co = coarse[p];
         src += co.top * stride + co.left;
     }
-    fft_upsample<N1, N2, F1, F2>(src, stride, rsm, twn, twf,
-                                 refined + (long long)blockIdx.x * refined_stride + out_off);
+    fft_upsample<N1, N2, F1, F2, UpsampleGeom<N1, N2, F1, F2>::CB>(
+        src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off);
 }
 
 // refinement (N, F = 2 N) pairs that are compiled: N, N1, N2, F1, F2
@@ -693,7 +685,7 @@ bool spec_refine_supported(int n, int f, int& smem)
     if (f != 2) return false;
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                \
     if (n == NN) {                                        \
-        smem = fft_upsample_smem<A, B, C, D>();           \
+        smem = UpsampleGeom<A, B, C, D>::smem;           \
         return smem <= 227 * 1024;                        \
     }
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
@@ -709,7 +701,7 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
 {
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                     \
     if (n == NN) {                                                                             \
-        spec_refine_kernel<A, B, C, D><<<blocks, kThreads, fft_upsample_smem<A, B, C, D>(), st>>>( \
+        spec_refine_kernel<A, B, C, D><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
             base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride,  \
             out_off);                                                                          \
         return cudaGetLastError();                                                             \

@@ -112,25 +112,13 @@ double check_upsample(std::mt19937& g)
     for (int y = 0; y < N; ++y) {
         for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(X.data() + y * N, 1, n2, twn.data());
         for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(X.data() + y * N, 1, k1);
-        for (int pp = 0; pp < F; ++pp) {
-            float w;
-            const int k = pad_source<N, F>(freq_at<F1, F2>(pp), w);
-            const float2 v = X[y * N + pos_of<N1, N2>(k)];
-            Y[y * F + pp] = make_float2(w * v.x, w * v.y);
-        }
-        for (int k1 = 0; k1 < F1; ++k1) step_b<F1, F2, 1>(Y.data() + y * F, 1, k1);
+        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(X.data() + y * N, 1, Y.data() + y * F, 1, k1);
         for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(Y.data() + y * F, 1, n2, twf.data());
     }
     for (int x = 0; x < F; ++x) {
         for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(Y.data() + x, F, n2, twn.data());
         for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(Y.data() + x, F, k1);
-        for (int yy = 0; yy < F; ++yy) {
-            float w;
-            const int k = pad_source<N, F>(freq_at<F1, F2>(yy), w);
-            const float2 v = Y[pos_of<N1, N2>(k) * F + x];
-            C[yy * F + x] = make_float2(w * v.x, w * v.y);
-        }
-        for (int k1 = 0; k1 < F1; ++k1) step_b<F1, F2, 1>(C.data() + x, F, k1);
+        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(Y.data() + x, F, C.data() + x, F, k1);
         for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(C.data() + x, F, n2, twf.data());
     }
     // direct: out = |A X A^T|, A[i][n] = D_N(i / f - n)
