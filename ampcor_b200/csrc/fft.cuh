@@ -313,6 +313,20 @@ HD void inv_a(float2* base, int es, int n2, const float2* tw)
     for (int n1 = 0; n1 < N1; ++n1) base[(N2 * n1 + n2) * es] = a[n1];
 }
 
+// inv_a whose natural-order outputs go to store(n, value) instead of back into the tile
+template <int N1, int N2, class Store>
+HD void inv_a_store(const float2* base, int es, int n2, const float2* tw, Store store)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) a[k1] = base[(N2 * k1 + n2) * es];
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmulc(a[k1], tw[n2 * k1]);
+    Dft<N1, 1>::run(a);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) store(N2 * n1 + n2, a[n1]);
+}
+
 // position of frequency k in the permuted spectrum, and the frequency at position p
 template <int N1, int N2>
 HD int pos_of(int k) { return N2 * (k % N1) + k / N1; }

@@ -335,17 +335,18 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
             if (cc < nc) fft::step_b_pad<N1, N2, F1, F2>(Y + c0 + cc, RSF, X + cc, CBS, t / CB);
         }
         __syncthreads();
+        // the last step writes the amplitudes of its outputs (rows n of column c0 + cc) straight
+        // to global memory; lanes take consecutive columns, so the stores coalesce
         for (int t = tid; t < CB * F2; t += kThreads) {
             const int cc = t % CB;
-            if (cc < nc) fft::inv_a<F1, F2>(X + cc, CBS, t / CB, twf);
-        }
-        __syncthreads();
-        for (int y = warp; y < F; y += kWarps)
-            for (int cc = lane; cc < nc; cc += 32) {
-                const float2 v = X[y * CBS + cc];
-                const float re = v.x * scale, im = v.y * scale;
-                out[(long long)y * F + c0 + cc] = sqrtf(re * re + im * im);
+            if (cc < nc) {
+                float* col = out + c0 + cc;
+                fft::inv_a_store<F1, F2>(X + cc, CBS, t / CB, twf, [&](int n, float2 v) {
+                    const float re = v.x * scale, im = v.y * scale;
+                    col[(long long)n * F] = sqrtf(re * re + im * im);
+                });
             }
+        }
         __syncthreads();
     }
 }

@@ -104,7 +104,7 @@ double check_upsample(std::mt19937& g)
 {
     constexpr int N = N1 * N2, F = F1 * F2, f = F / N;
     std::normal_distribution<double> nd;
-    std::vector<float2> X(N * N), Y(N * F), C(F * F), twn(N), twf(F);
+    std::vector<float2> X(N * N), Y(N * F), C(F * F), Out(F * F), twn(N), twf(F);
     for (int m = 0; m < N; ++m) twn[m] = make_float2((float)cos(2 * M_PI * m / N), (float)-sin(2 * M_PI * m / N));
     for (int m = 0; m < F; ++m) twf[m] = make_float2((float)cos(2 * M_PI * m / F), (float)-sin(2 * M_PI * m / F));
     for (auto& v : X) v = make_float2((float)nd(g), (float)nd(g));
@@ -119,7 +119,8 @@ double check_upsample(std::mt19937& g)
         for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(Y.data() + x, F, n2, twn.data());
         for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(Y.data() + x, F, k1);
         for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(Y.data() + x, F, C.data() + x, F, k1);
-        for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(C.data() + x, F, n2, twf.data());
+        for (int n2 = 0; n2 < F2; ++n2)
+            inv_a_store<F1, F2>(C.data() + x, F, n2, twf.data(), [&](int n, float2 v) { Out[n * F + x] = v; });
     }
     // direct: out = |A X A^T|, A[i][n] = D_N(i / f - n)
     std::vector<double> A(F * N);
@@ -138,7 +139,7 @@ double check_upsample(std::mt19937& g)
             double sr = 0, si = 0;
             for (int n = 0; n < N; ++n) { sr += Tr[i * N + n] * A[j * N + n]; si += Ti[i * N + n] * A[j * N + n]; }
             const double ref = hypot(sr, si);
-            const float2 v = C[i * F + j];
+            const float2 v = Out[i * F + j];
             const double got = hypot((double)v.x, (double)v.y) / ((double)N * N);
             err = fmax(err, fabs(got - ref));
             mag = fmax(mag, ref);
