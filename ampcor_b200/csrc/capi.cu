@@ -239,6 +239,8 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     off += 256;
     g.off_inv = (int)off;  // the placement statistics, prefetched with the tiles
     off = up(off + (long)g.C * g.C * 4, 16);
+    g.off_gam = (int)off;  // the normalised surface
+    off = up(off + (long)g.C * g.C * 4, 16);
     if (off > 227L * 1024) {
         err = "tile geometry too large for the spectral form";
         return false;

@@ -398,13 +398,14 @@ HD void step_b_pad(const float2* src, int src_es, float2* dst, int dst_es, int k
 // holding t + i r: the window t in the real parts, the chip r in the imaginary parts, zero
 // outside them, centred on the way in as `centre` says.  Rows at and past rows_in are all zero.
 // neg[p] = neg_pos(p) for p < N.
-// Afterwards, for u < rows_out and v < N, Z[u][v].x holds 4 N^2 sum_ij r(i, j) t(u + i, v + j)
+// The correlation goes to store(u, v, value) for u < rows_out and v < N: value.x is
+// 4 N^2 sum_ij r(i, j) t(u + i, v + j)
 // (circular indices, which never wrap for the placements of a window of at most N samples).  The
 // tasks of each phase are spread over the nt threads; sync() separates the phases
 // (__syncthreads on the device).
-template <int N1, int N2, class Sync>
+template <int N1, int N2, class Sync, class Store>
 HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
-                       const int* neg, const Centre& centre, int tid, int nt, Sync sync)
+                       const int* neg, const Centre& centre, int tid, int nt, Sync sync, Store store)
 {
     constexpr int N = N1 * N2;
     // forward along rows (centring the tile on the way in): lanes take consecutive rows
@@ -460,9 +461,10 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
         step_b<N1, N2, 1>(Z + y * RS, 1, k1);
     }
     sync();
+    // the last step hands its outputs to store(u, v, value) instead of writing them back
     for (int t = tid; t < rows_out * N2; t += nt) {
         const int y = t % rows_out, n2 = t / rows_out;
-        inv_a<N1, N2>(Z + y * RS, 1, n2, tw);
+        inv_a_store<N1, N2>(Z + y * RS, 1, n2, tw, [&](int n, float2 v) { store(y, n, v); });
     }
     sync();
 }

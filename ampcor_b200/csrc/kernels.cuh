@@ -209,7 +209,7 @@ struct SpecGeom {
     int R, W, C;      // chip, window, placements per axis
     int N, N1, N2;    // transform length and its two register radices
     int RS;           // tile row stride (complex samples)
-    int off_z, off_tw, off_neg, off_red, off_inv;  // shared-memory byte offsets
+    int off_z, off_tw, off_neg, off_red, off_inv, off_gam;  // shared-memory byte offsets
     int smem_bytes;
 };
 

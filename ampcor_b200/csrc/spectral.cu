@@ -89,34 +89,17 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
 constexpr float kSpecErr = 1e-6f;
 constexpr float kSpecTol = 4e-6f;
 
-// Normalised surface -> first maximum (valid in every thread); optional copies of the surface.
-// The surface is built in the imaginary parts of the placement rows of the tile; inv holds
-// 1/sigma_box of the placements in shared memory (row stride C).
-__device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const float* inv,
-                             float inv_sigma, double mean_c, float tnorm, const float* chip,
+// The normalised surface G (C x C in shared memory, formed by the last transform step) -> its
+// first maximum (valid in every thread) and optional copies.  On entry every thread holds the
+// maximum of the placements it formed whose transform bound is tight, and whether it formed any
+// whose bound is loose (flagged); inv holds 1/sigma_box of the placements (row stride C).
+__device__ void spec_surface(float* G, double* red, const SpecGeom& g, const float* inv,
+                             float inv_sigma, double mean_c, float ebox, const float* chip,
                              long long cs, const float* win, long long ws, float* out1, float* out2,
-                             float& bv, int& bi)
+                             float& bv, int& bi, int flagged)
 {
-    const int C = g.C, RS = g.RS, R = g.R;
+    const int C = g.C, R = g.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const float scale = (float)(1.0 / (4.0 * (double)g.N * (double)g.N));
-    const float ebox = kSpecErr * tnorm;
-    bv = -INFINITY;
-    bi = INT_MAX;
-    int flagged = 0;
-    for (int u = warp; u < C; u += kWarps) {
-        for (int v = lane; v < C; v += 32) {
-            const int idx = u * C + v;
-            float2* z = Z + u * RS + v;
-            const float inv_box = inv[idx];
-            const float gv = z->x * scale * inv_box * inv_sigma;
-            z->y = gv;
-            if (ebox * inv_box > kSpecTol)
-                flagged = 1;
-            else
-                better(bv, bi, gv, idx);
-        }
-    }
     block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
     if (__syncthreads_or(flagged)) {
         // direct FP32 numerators where the transform's bound is loose and the value matters: one
@@ -128,8 +111,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
             const int u = idx / C, v = idx - u * C;
             const float inv_box = inv[idx];
             const float e = ebox * inv_box;
-            float* gp = &Z[u * RS + v].y;
-            if (!(e > kSpecTol) || !(all || *gp + e >= bv)) continue;
+            if (!(e > kSpecTol) || !(all || G[idx] + e >= bv)) continue;
             float acc = 0.0f;
             for (int i = 0; i < R; ++i)
                 for (int j = lane; j < R; j += 32) {
@@ -139,7 +121,7 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
             const double num = warp_sum((double)acc);
             const float gv = (float)num * inv_box * inv_sigma;
             __syncwarp();
-            if (lane == 0) *gp = gv;
+            if (lane == 0) G[idx] = gv;
             better(wv, wi, gv, idx);
         }
         // every flagged placement that could win has its exact value now; the others stay below
@@ -148,12 +130,10 @@ __device__ void spec_surface(float2* Z, double* red, const SpecGeom& g, const fl
         block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
     }
     if (out1 || out2) {
-        for (int u = warp; u < C; u += kWarps) {
-            for (int v = lane; v < C; v += 32) {
-                const float gv = Z[u * RS + v].y;
-                if (out1) out1[u * C + v] = gv;
-                if (out2) out2[u * C + v] = gv;
-            }
+        for (int idx = threadIdx.x; idx < C * C; idx += kThreads) {
+            const float gv = G[idx];
+            if (out1) out1[idx] = gv;
+            if (out2) out2[idx] = gv;
         }
     }
 }
@@ -181,6 +161,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
     double* red = reinterpret_cast<double*>(ssm + g.off_red);
     float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
+    float* G = reinterpret_cast<float*>(ssm + g.off_gam);
     float* Zf = reinterpret_cast<float*>(Z);
     const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
     const long long is = inv.off ? inv.stride : C;
@@ -254,14 +235,30 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
     const fft::Centre centre{(float)mean_w, W, mc_hi, mc_lo, R};
 
-    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, centre, tid, kThreads, BlockSync{});
+    // the last transform step forms gamma of every placement straight from its outputs and keeps
+    // this thread's maximum of those whose transform bound is tight
+    const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
+    const float ebox = kSpecErr * (float)sqrt(st);
+    float bv = -INFINITY;
+    int bi = INT_MAX;
+    int flagged = 0;
+    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, centre, tid, kThreads, BlockSync{},
+                                [&](int u, int v, float2 val) {
+                                    if (v < C) {
+                                        const int idx = u * C + v;
+                                        const float inv_box = invs[idx];
+                                        const float gv = val.x * scale * inv_box * inv_sigma;
+                                        G[idx] = gv;
+                                        if (ebox * inv_box > kSpecTol)
+                                            flagged = 1;
+                                        else
+                                            better(bv, bi, gv, idx);
+                                    }
+                                });
 
-    float bv;
-    int bi;
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
-    spec_surface(Z, red, g, invs, inv_sigma, mean_c, (float)sqrt(st), chip, cs, win, ws, gam, surf,
-                 bv, bi);
+    spec_surface(G, red, g, invs, inv_sigma, mean_c, ebox, chip, cs, win, ws, gam, surf, bv, bi, flagged);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;
         if (out.stage == 0) {
