@@ -239,34 +239,18 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     off += 256;
     g.off_inv = (int)off;  // the placement statistics, prefetched with the tiles
     off = up(off + (long)g.C * g.C * 4, 16);
-    g.off_gam = (int)off;  // the normalised surface
-    off = up(off + (long)g.C * g.C * 4, 16);
-    if (off > 227L * 1024) {
+    g.off_gam = (int)off;  // the normalised surface; before the last step, the statistics' scratch
+    const long limit = 227L * 1024;
+    // column sums (two floats a placement row and window column) past the tile's imaginary parts
+    const long over = std::max<long>(0, 2L * g.C * g.W - (long)g.N * g.RS) * 4;
+    g.nseg = std::max(1, kThreads / g.W);
+    while (g.nseg > 1 && off + 32L * g.nseg * g.W + over > limit) --g.nseg;
+    off = up(off + std::max<long>((long)g.C * g.C * 4, 32L * g.nseg * g.W + over), 16);
+    if (off > limit) {
         err = "tile geometry too large for the spectral form";
         return false;
     }
     g.smem_bytes = (int)off;
-    return true;
-}
-
-// placement statistics kernel: a prefix scratch row per warp (FP64) and float column-sum slices
-// of SU placement rows, sized so that two CTAs fit on an SM
-bool plan_box(int R, int W, BoxGeom& g, std::string& err)
-{
-    std::memset(&g, 0, sizeof(g));
-    g.R = R;
-    g.W = W;
-    g.C = W - R + 1;
-    g.VS = W + 1;
-    g.nb = std::max(1, kThreads / W);
-    const long scratch = (long)kWarps * 2 * (W + 1) * 8;
-    const long row_bytes = 2L * g.VS * 4;
-    g.SU = (int)std::min<long>(g.C, (113L * 1024 - scratch) / row_bytes);
-    if (g.SU < 1) {
-        err = "window too wide for the placement statistics kernel";
-        return false;
-    }
-    g.smem_bytes = (int)(scratch + g.SU * row_bytes);
     return true;
 }
 
@@ -439,7 +423,6 @@ struct ampcor_handle {
     // correlation form (kFormPlain, kFormTensor, kFormSpectral)
     int form = 0;
     SpecGeom spc{}, spf{};
-    BoxGeom bxc{}, bxf{};
     // tensor-core zoom (both the tensor-core and the spectral forms), when Zm fits
     bool zoom_tc = false;
     ZoomTcGeom ztc{};
@@ -731,8 +714,8 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
     if (!shared) detect(src.tgt_base, src.tgt_count, amp_tgt);
     CK(h, cudaGetLastError(), "launching the detection kernel");
     // coarse box statistics once per raster where the windows tile a raster (they overlap), else
-    // per pair in the chunk loop
-    InvSource inv_c{h->d_inv_c, nullptr, 0};
+    // inside the correlation kernel from the window it holds (as for every fine window)
+    InvSource inv_c{nullptr, nullptr, 0};
     const long long rows = src.tgt_lines - h->R + 1;
     const bool raster_stats = src.tgt_lines > 0 && rows > 0 && src.tgt_stride <= 12288;
     if (raster_stats) {
@@ -755,13 +738,7 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
     for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
-        cudaEvent_t a = mark(h, st);
-        if (!raster_stats) {
-            box_stats_kernel<<<n, kThreads, h->bxc.smem_bytes, st>>>(cs, c0, n, src.ref_off, h->bxc, h->d_inv_c);
-            CK(h, cudaGetLastError(), "launching the coarse statistics kernel");
-        }
         cudaEvent_t b = mark(h, st);
-        keep(h, 3, a, b, raster_stats ? 0 : 1);
         CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, inv_c,
                           reinterpret_cast<const float2*>(h->d_tw_c),
                           SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
@@ -783,13 +760,9 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
                                                                h->d_refined, h->refined_stride);
             CK(h, cudaGetLastError(), "launching the refinement kernel");
         }
-        cudaEvent_t d = mark(h, st);
-        keep(h, 1, c, d, h->refine_fft ? 2 : 1);
-        box_stats_kernel<<<n, kThreads, h->bxf.smem_bytes, st>>>(fs, c0, n, src.ref_off, h->bxf, h->d_inv_f);
-        CK(h, cudaGetLastError(), "launching the fine statistics kernel");
         cudaEvent_t e = mark(h, st);
-        keep(h, 4, d, e);
-        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{h->d_inv_f, nullptr, 0},
+        keep(h, 1, c, e, h->refine_fft ? 2 : 1);
+        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
                           reinterpret_cast<const float2*>(h->d_tw_f),
                           SpecOut{1, 0, nullptr, nullptr, h->d_fine_out, h->d_gam, refined_surfaces}),
            "launching the spectral fine correlation");
@@ -885,8 +858,7 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     {
         const char* env = std::getenv("AMPCOR_FORM");
         std::string terr;
-        const bool spec_ok = plan_spec(h->R, h->W, h->spc, terr) && plan_spec(h->Rf, h->Wf, h->spf, terr) &&
-                             plan_box(h->R, h->W, h->bxc, terr) && plan_box(h->Rf, h->Wf, h->bxf, terr);
+        const bool spec_ok = plan_spec(h->R, h->W, h->spc, terr) && plan_spec(h->Rf, h->Wf, h->spf, terr);
         const bool tc_ok = plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
         h->form = spec_ok ? kFormSpectral : tc_ok ? kFormTensor : kFormPlain;
         if (p->flags & AMPCOR_FLAG_PLAIN_FP32) h->form = kFormPlain;
@@ -1269,8 +1241,7 @@ int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
             return fail(h, AMPCOR_E_SHAPE, "this geometry has no tensor-core form: " + terr);
     } else if (form == kFormSpectral) {
         std::string terr;
-        if (!plan_spec(h->R, h->W, h->spc, terr) || !plan_spec(h->Rf, h->Wf, h->spf, terr) ||
-            !plan_box(h->R, h->W, h->bxc, terr) || !plan_box(h->Rf, h->Wf, h->bxf, terr))
+        if (!plan_spec(h->R, h->W, h->spc, terr) || !plan_spec(h->Rf, h->Wf, h->spf, terr))
             return fail(h, AMPCOR_E_SHAPE, "this geometry has no spectral form: " + terr);
     } else if (form != kFormPlain && form != -1) {
         return fail(h, AMPCOR_E_ARG, "form must be -1, 0, 1 or 2");

@@ -210,17 +210,11 @@ struct SpecGeom {
     int N, N1, N2;    // transform length and its two register radices
     int RS;           // tile row stride (complex samples)
     int off_z, off_tw, off_neg, off_red, off_inv, off_gam;  // shared-memory byte offsets
-    int smem_bytes;
-};
-
-// placement statistics of one surface per CTA (512 threads, two CTAs per SM): column sums over R
-// rows for a slice of SU placement rows at a time (nb blocks of placement rows per column), then
-// FP64 prefix sums along each row
-struct BoxGeom {
-    int R, W, C;
-    int SU;        // placement rows per slice
-    int nb;        // blocks of placement rows per column
-    int VS;        // row stride of the column-sum slices (floats), W + 1
+    // placement statistics computed in the kernel (no InvSource given): nseg threads per window
+    // column, their FP64 partial sums (4 nseg W doubles) at off_gam (the surface buffer, idle
+    // until the last transform step), the column sums in the tile's imaginary parts and, past the
+    // tile, right after the partial sums
+    int nseg;
     int smem_bytes;
 };
 
@@ -267,8 +261,6 @@ struct InvSource {
     const long long* off;
     long long stride;
 };
-__global__ void box_stats_kernel(SpecSource s, long long pair0, long long pairs,
-                                 const long long* valid, BoxGeom g, float* inv);
 
 // the transform lengths that are compiled, with their radices
 bool spec_radices(int n, int& n1, int& n2);

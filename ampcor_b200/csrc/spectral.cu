@@ -10,9 +10,11 @@
 // geometry (64^2 chips, 128^2 windows).
 //
 // Around it: the amplitudes of each raster are detected once (detect_kernel; neighbouring
-// windows overlap, so every sample is shared by many pairs), the FP64 placement statistics of a
-// chunk come from their own kernel (box_stats_kernel, two CTAs per SM, every thread busy), and the
-// correlation kernel takes float amplitudes through asynchronous copies.
+// windows overlap, so every sample is shared by many pairs) and the correlation kernel takes float
+// amplitudes through asynchronous copies.  The placement statistics (1/sigma of every window box)
+// come from the window while it sits in shared memory (spec_box_stats), or, for the coarse stage
+// of windows that tile a raster, from FP64 sums over the whole raster (box_vsum_kernel,
+// box_inv_kernel).
 //
 // Accuracy.  The window is centred on its mean before the transform (sum r' = 0, so the
 // numerators keep their value) and the twiddles are correctly rounded, which keeps the transform
@@ -89,6 +91,185 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
 constexpr float kSpecErr = 1e-6f;
 constexpr float kSpecTol = 4e-6f;
 
+// Scratch of the placement statistics while the chip waits in registers: slot k is the imaginary
+// part of tile sample k, and past the tile's nz samples it continues in the tail buffer.
+struct StatSlots {
+    float* z;  // imaginary part of tile sample 0 (slots 2 floats apart)
+    float* tail;
+    int nz;
+    __device__ __forceinline__ float* at(int k) const { return k < nz ? z + 2 * k : tail + (k - nz); }
+};
+
+__device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
+{
+    const float var = (float)(b2 - b1 * b1 * rcells);
+    return var > 0.0f ? __frsqrt_rn(var) : 0.0f;
+}
+
+// error-free sum of two floats (Knuth's two-sum): hi + lo == a + b exactly
+__device__ __forceinline__ void two_sum(float a, float b, float& hi, float& lo)
+{
+    hi = a + b;
+    const float bb = hi - a;
+    lo = (a - (hi - bb)) + (b - bb);
+}
+
+// 1/sigma_box of every placement from the window in the tile's real parts (rows RS apart), the
+// values shifted by sx (the window mean: the box variance does not change and the column sums
+// keep their digits).  sigma^2 = S2 - S1^2 / R^2 over the R x R box, its sum of squared deviations
+// from its mean: the target variance of correlate.cu:196-309, whose box mean comes from the
+// summed-area table (tgtStats.cu).
+//
+// Column sums V(u, x) over window rows [u, u + R), nseg threads per column: thread s sums band s
+// of the first placement's rows (FP32 runs of 8 rows added in FP64) and the slides
+// delta(i) = t(i + R) - t(i) of its share of the placement rows (FP32: a slide is small next to a
+// column sum); after one exchange (part, FP64) each thread starts its share at V(0) plus the
+// earlier shares' slides, carries the running sums as float pairs (two-sum, no rounding) and
+// writes V(u, x) of its rows as floats into the slots (V1 at slot u W + x, V2 at C W + u W + x).
+// Then one warp per placement row (two rows at a time) forms the box sums
+// S(v) = sum_{x in [v, v + R)} V(x): S(0) as an FP64 warp sum, the others as S(0) plus an FP32 scan
+// of V(v + R) - V(v) across the lanes.  Conversions between float and double are few: they run
+// at a fraction of the FP32 rate.  Ends with a barrier.
+__device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float sx, StatSlots vs,
+                               double* part, float* invs)
+{
+    const int R = g.R, W = g.W, C = g.C, nseg = g.nseg, D = C - 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x = tid % W, s = tid / W;
+    auto tv = [&](int y) { return Z[y * RS + x].x - sx; };
+    constexpr int kRun = 8;
+    if (s < nseg) {
+        double b1 = 0.0, b2 = 0.0;
+        const int ya = s * R / nseg, yb = (s + 1) * R / nseg;
+        for (int y0 = ya; y0 < yb; y0 += kRun) {
+            float r1 = 0.0f, r2 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kRun; ++k)
+                if (y0 + k < yb) {
+                    const float t = tv(y0 + k);
+                    r1 += t;
+                    r2 = fmaf(t, t, r2);
+                }
+            b1 += (double)r1;
+            b2 += (double)r2;
+        }
+        float e1 = 0.0f, e2 = 0.0f;
+        for (int i = s * D / nseg, i1 = (s + 1) * D / nseg; i < i1; ++i) {
+            const float a = tv(i + R), b = tv(i);
+            e1 += a - b;
+            e2 = fmaf(a - b, a + b, e2);
+        }
+        part[(0 * nseg + s) * W + x] = b1;
+        part[(1 * nseg + s) * W + x] = b2;
+        part[(2 * nseg + s) * W + x] = (double)e1;
+        part[(3 * nseg + s) * W + x] = (double)e2;
+    }
+    __syncthreads();
+    if (s < nseg) {
+        double v1 = 0.0, v2 = 0.0;
+        for (int q = 0; q < nseg; ++q) {
+            v1 += part[(0 * nseg + q) * W + x];
+            v2 += part[(1 * nseg + q) * W + x];
+        }
+        for (int q = 0; q < s; ++q) {
+            v1 += part[(2 * nseg + q) * W + x];
+            v2 += part[(3 * nseg + q) * W + x];
+        }
+        float h1 = (float)v1, l1 = (float)(v1 - (double)h1);
+        float h2 = (float)v2, l2 = (float)(v2 - (double)h2);
+        const int i1 = (s + 1) * D / nseg;
+        constexpr int kB = 4;  // window rows read ahead of the running sums
+        for (int i0 = s * D / nseg; i0 < i1; i0 += kB) {
+            float a[kB], b[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                const int i = min(i0 + k, i1 - 1);
+                a[k] = tv(i + R);
+                b[k] = tv(i);
+            }
+#pragma unroll
+            for (int k = 0; k < kB; ++k)
+                if (i0 + k < i1) {
+                    *vs.at((i0 + k) * W + x) = h1 + l1;
+                    *vs.at((C + i0 + k) * W + x) = h2 + l2;
+                    float e;
+                    two_sum(h1, a[k] - b[k], h1, e);
+                    l1 += e;
+                    two_sum(h2, (a[k] - b[k]) * (a[k] + b[k]), h2, e);
+                    l2 += e;
+                }
+        }
+        if (s == nseg - 1) {
+            *vs.at(D * W + x) = h1 + l1;
+            *vs.at((C + D) * W + x) = h2 + l2;
+        }
+    }
+    __syncthreads();
+    const double rcells = 1.0 / ((double)R * (double)R);
+    for (int u = warp; u < C; u += 2 * kWarps) {
+        // rows u and u + kWarps; the second is row C - 1 again (not stored) past the end
+        const int uu[2] = {u, min(u + kWarps, C - 1)};
+        const bool keep2 = u + kWarps < C;
+        double s1[2], s2[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            float f1 = 0.0f, f2 = 0.0f;
+            for (int c = lane; c < R; c += 32) {
+                f1 += *vs.at(uu[r] * W + c);
+                f2 += *vs.at((C + uu[r]) * W + c);
+            }
+            s1[r] = (double)f1;
+            s2[r] = (double)f2;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                s1[r] += __shfl_xor_sync(kFull, s1[r], o);
+                s2[r] += __shfl_xor_sync(kFull, s2[r], o);
+            }
+        if (lane == 0) {
+            invs[uu[0] * C] = box_inv_of(s1[0], s2[0], rcells);
+            if (keep2) invs[uu[1] * C] = box_inv_of(s1[1], s2[1], rcells);
+        }
+        for (int j0 = 0; j0 < D; j0 += 32) {
+            const int j = j0 + lane;
+            float i1[2], i2[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                i1[r] = 0.0f;
+                i2[r] = 0.0f;
+                if (j < D) {
+                    i1[r] = *vs.at(uu[r] * W + j + R) - *vs.at(uu[r] * W + j);
+                    i2[r] = *vs.at((C + uu[r]) * W + j + R) - *vs.at((C + uu[r]) * W + j);
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                    const float y1 = __shfl_up_sync(kFull, i1[r], o);
+                    const float y2 = __shfl_up_sync(kFull, i2[r], o);
+                    if (lane >= o) {
+                        i1[r] += y1;
+                        i2[r] += y2;
+                    }
+                }
+            if (j < D) {
+                invs[uu[0] * C + j + 1] = box_inv_of(s1[0] + (double)i1[0], s2[0] + (double)i2[0], rcells);
+                if (keep2)
+                    invs[uu[1] * C + j + 1] = box_inv_of(s1[1] + (double)i1[1], s2[1] + (double)i2[1], rcells);
+            }
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                s1[r] += (double)__shfl_sync(kFull, i1[r], 31);
+                s2[r] += (double)__shfl_sync(kFull, i2[r], 31);
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // The normalised surface G (C x C in shared memory, formed by the last transform step) -> its
 // first maximum (valid in every thread) and optional copies.  On entry every thread holds the
 // maximum of the placements it formed whose transform bound is tight, and whether it formed any
@@ -163,14 +344,25 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
     float* G = reinterpret_cast<float*>(ssm + g.off_gam);
     float* Zf = reinterpret_cast<float*>(Z);
-    const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
+    // placement statistics: given (inv.base), else computed here from the window
+    const float* inv_b = !inv.base ? nullptr : inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * C * C;
     const long long is = inv.off ? inv.stride : C;
     const float* chip = spec_chip(src, pair0, blockIdx.x);
     const float* win = spec_win(src, pair0, blockIdx.x);
     const long long cs = src.chip_stride, ws = src.win_stride;
 
-    // window amplitudes -> real parts, chip amplitudes -> imaginary parts (4-byte asynchronous
-    // copies, all in flight at once), zeros elsewhere
+    // The chip goes to registers (its loads in flight with the window's), the window amplitudes
+    // to the real parts of the tile by 4-byte asynchronous copies, zeros to the other real parts.
+    // The imaginary parts are the placement statistics' scratch until the chip is stored there.
+    constexpr int JN = (N + kWarps - 1) / kWarps, IN = (N + 31) / 32;
+    float cr[JN][IN];
+#pragma unroll
+    for (int j = 0; j < JN; ++j)
+#pragma unroll
+        for (int i = 0; i < IN; ++i) {
+            const int y = warp + kWarps * j, x = lane + 32 * i;
+            cr[j][i] = y < R && x < R ? __ldg(chip + y * cs + x) : 0.0f;
+        }
     for (int y = warp; y < N; y += kWarps) {
         float* zr = Zf + 2 * y * RS;
         for (int x = lane; x < N; x += 32) {
@@ -178,15 +370,12 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
                 cp_async4(zr + 2 * x, win + y * ws + x);
             else
                 zr[2 * x] = 0.0f;
-            if (y < R && x < R)
-                cp_async4(zr + 2 * x + 1, chip + y * cs + x);
-            else
-                zr[2 * x + 1] = 0.0f;
         }
     }
-    // the placement statistics land in shared memory while the transform runs
-    for (int u = warp; u < C; u += kWarps)
-        for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
+    // given placement statistics land in shared memory with the window
+    if (inv_b)
+        for (int u = warp; u < C; u += kWarps)
+            for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
     for (int k = tid; k < N; k += kThreads) {
         tw[k] = __ldg(tw_g + k);
         neg[k] = fft::neg_pos<N1, N2>(k);
@@ -207,18 +396,22 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         for (int y = warp; y < W; y += kWarps) {
             const float2* zr = Z + y * RS;
             for (int x = lane; x < W; x += 32) {
-                const float2 z = zr[x];
-                sw += z.x;
-                sw2 = fmaf(z.x, z.x, sw2);
-                if (y < R && x < R) {
-                    const float yk = z.y - cc;
-                    const float tk = sc + yk;
-                    cc = (tk - sc) - yk;
-                    sc = tk;
-                    sc2 = fmaf(z.y, z.y, sc2);
-                }
+                const float t = zr[x].x;
+                sw += t;
+                sw2 = fmaf(t, t, sw2);
             }
         }
+#pragma unroll
+        for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int i = 0; i < IN; ++i) {
+                const float r = cr[j][i];
+                const float yk = r - cc;
+                const float tk = sc + yk;
+                cc = (tk - sc) - yk;
+                sc = tk;
+                sc2 = fmaf(r, r, sc2);
+            }
         acc4[0] = (double)sc - (double)cc;
         acc4[1] = sc2;
         acc4[2] = sw;
@@ -234,6 +427,20 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
     const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
     const fft::Centre centre{(float)mean_w, W, mc_hi, mc_lo, R};
+    if (!inv_b) {
+        double* part = reinterpret_cast<double*>(ssm + g.off_gam);
+        const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
+        spec_box_stats(Z, RS, g, centre.sx, vs, part, invs);
+    }
+    // the chip into the imaginary parts, zeros around it
+#pragma unroll
+    for (int j = 0; j < JN; ++j)
+#pragma unroll
+        for (int i = 0; i < IN; ++i) {
+            const int y = warp + kWarps * j, x = lane + 32 * i;
+            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = cr[j][i];
+        }
+    __syncthreads();
 
     // the last transform step forms gamma of every placement straight from its outputs and keeps
     // this thread's maximum of those whose transform bound is tight
@@ -544,118 +751,6 @@ box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, lon
     }
 }
 
-// exclusive prefix sums (FP64) of the n floats of rows a and b into Pa and Pb [0 .. n] (element n
-// the total), the two scans interleaved; one warp
-__device__ void warp_prefix2_f(const float* a, const float* b, int n, double* Pa, double* Pb)
-{
-    const int lane = threadIdx.x & 31;
-    const int per = (n + 31) / 32;
-    const int beg = min(lane * per, n), end = min(beg + per, n);
-    double la = 0.0, lb = 0.0;
-    for (int k = beg; k < end; ++k) {
-        la += (double)a[k];
-        lb += (double)b[k];
-    }
-    double ia = la, ib = lb;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double ya = __shfl_up_sync(kFull, ia, o);
-        const double yb = __shfl_up_sync(kFull, ib, o);
-        if (lane >= o) {
-            ia += ya;
-            ib += yb;
-        }
-    }
-    double ra = ia - la, rb = ib - lb;
-    for (int k = beg; k < end; ++k) {
-        Pa[k] = ra;
-        Pb[k] = rb;
-        ra += (double)a[k];
-        rb += (double)b[k];
-    }
-    if (end == n && beg < n) {
-        Pa[n] = ra;
-        Pb[n] = rb;
-    }
-    __syncwarp();
-}
-
-// 1/sqrt(sum_box t^2 - (sum_box t)^2 / R^2) of every placement of a chunk-local pair (0 for a flat
-// box): the summed-area statistics of tgtStats.cu:139-162 and sat.cu:81-149.  Column sums over R
-// rows (compensated FP32 for the first box of a block of placement rows, then slid down in FP64,
-// nb blocks per column) straight from the window in L2 / HBM, kept as floats for SU placement
-// rows at a time; then FP64 prefix sums along each placement row (a warp per row, its own
-// scratch) and the box of every placement from two prefix differences.  Two CTAs per SM.
-__global__ void __launch_bounds__(kThreads, 2)
-box_stats_kernel(SpecSource s, long long pair0, long long pairs, const long long* valid, BoxGeom g,
-                 float* inv)
-{
-    extern __shared__ __align__(16) double bsm[];
-    if (blockIdx.x >= pairs) return;
-    if (valid[pair0 + blockIdx.x] < 0) return;
-    const float* win = spec_win(s, pair0, blockIdx.x);
-    const long long ws = s.win_stride;
-    const int R = g.R, W = g.W, C = g.C, VS = g.VS, SU = g.SU, nb = g.nb;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* P1 = bsm + warp * 2 * (W + 1);  // this warp's prefix scratch
-    double* P2 = P1 + (W + 1);
-    float* V1 = reinterpret_cast<float*>(bsm + kWarps * 2 * (W + 1));
-    float* V2 = V1 + SU * VS;
-    float* out = inv + (long long)blockIdx.x * C * C;
-    const double rcells = 1.0 / ((double)R * (double)R);
-    constexpr int kBatch = 8;  // window rows loaded before they are summed
-    for (int u0 = 0; u0 < C; u0 += SU) {
-        const int nu = min(SU, C - u0);
-        const int B = (nu + nb - 1) / nb;
-        for (int t = tid; t < W * nb; t += kThreads) {
-            const int x = t % W, ub = t / W;
-            const int ua = u0 + ub * B, ue = min(ua + B, u0 + nu);
-            if (ua >= ue) continue;
-            const float* col = win + x + (long long)ua * ws;
-            float s1 = 0.0f, c1 = 0.0f, s2 = 0.0f, c2 = 0.0f;
-            for (int i0 = 0; i0 < R; i0 += kBatch) {
-                float tb[kBatch];
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) tb[k] = i0 + k < R ? __ldg(col + (long long)(i0 + k) * ws) : 0.0f;
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) {
-                    const float tv = tb[k];
-                    const float y1 = tv - c1, t1 = s1 + y1;
-                    c1 = (t1 - s1) - y1;
-                    s1 = t1;
-                    const float y2 = tv * tv - c2, t2 = s2 + y2;
-                    c2 = (t2 - s2) - y2;
-                    s2 = t2;
-                }
-            }
-            col = win + x;
-            double d1 = (double)s1 - (double)c1, d2 = (double)s2 - (double)c2;
-            for (int u = ua; u < ue; ++u) {
-                V1[(u - u0) * VS + x] = (float)d1;
-                V2[(u - u0) * VS + x] = (float)d2;
-                if (u + 1 < ue) {
-                    const double a = __ldg(col + (long long)(u + R) * ws);
-                    const double b = __ldg(col + (long long)u * ws);
-                    d1 += a - b;
-                    d2 += a * a - b * b;
-                }
-            }
-        }
-        __syncthreads();
-        for (int r = warp; r < nu; r += kWarps) {
-            warp_prefix2_f(V1 + r * VS, V2 + r * VS, W, P1, P2);
-            for (int v = lane; v < C; v += 32) {
-                const double b1 = P1[v + R] - P1[v];
-                const double b2 = P2[v + R] - P2[v];
-                const float var = (float)(b2 - b1 * b1 * rcells);
-                out[(u0 + r) * C + v] = var > 0.0f ? __frsqrt_rn(var) : 0.0f;
-            }
-            __syncwarp();
-        }
-        __syncthreads();
-    }
-}
-
 bool spec_radices(int n, int& n1, int& n2)
 {
 #define AMPCOR_SPEC_CASE(NN, A, B) \
@@ -712,9 +807,7 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
 cudaError_t spec_set_smem_limits()
 {
     const int limit = 227 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(box_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(box_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    cudaError_t e = cudaFuncSetAttribute(box_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D) \
     if (e == cudaSuccess)                  \
         e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);

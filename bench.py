@@ -324,8 +324,7 @@ def run_b200(args):
             work = {
                 "coarse_correlation": ("hbm", 4.0 * (W * W + R * R + C * C)),
                 "refinement": ("hbm", 8.0 * (R * R + E * E) + 4.0 * (Rf * Rf + Wf * Wf)),
-                "fine_statistics": ("hbm", 4.0 * (Wf * Wf + Cf * Cf)),
-                "fine_correlation": ("hbm", 4.0 * (Wf * Wf + Rf * Rf + 2 * Cf * Cf)),
+                "fine_correlation": ("hbm", 4.0 * (Wf * Wf + Rf * Rf + Cf * Cf)),
             }
         else:
             work = {
@@ -342,8 +341,7 @@ def run_b200(args):
             "refinement": {"spectral": "spec_refine_kernel (chip + window)"}.get(worker.form, "refine_kernel"),
             "coarse_statistics": {"spectral": "detect_kernel + box_vsum_kernel + box_inv_kernel (per raster)"}
             .get(worker.form, "window_stats_cplx_kernel"),
-            "fine_statistics": {"spectral": "box_stats_kernel (fine)"}
-            .get(worker.form, "window_stats_real_kernel"),
+            "fine_statistics": "window_stats_real_kernel",
             "zoom": "tc_zoom_kernel (zoom_kernel where Zm exceeds the tensor memory)",
         }
         peaks = {}
