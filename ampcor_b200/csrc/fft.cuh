@@ -392,6 +392,25 @@ HD void step_b_pad(const float2* src, int src_es, float2* dst, int dst_es, int k
     for (int j = 0; j < F2; ++j) dst[(F2 * k1 + j) * dst_es] = a[j];
 }
 
+// f(y, j) for every y < rows and j < J, spread over nt threads (thread tid first) in the order
+// t = j rows + y, so that lanes take consecutive y; the runtime division happens once per pass,
+// not once per task
+template <class F>
+HD void row_tasks(int rows, int J, int tid, int nt, F f)
+{
+    const int dj = nt / rows, dy = nt - dj * rows;
+    int j = tid / rows, y = tid - j * rows;
+    while (j < J) {
+        f(y, j);
+        y += dy;
+        j += dj;
+        if (y >= rows) {
+            y -= rows;
+            ++j;
+        }
+    }
+}
+
 // ---- the 2-D correlation of one tile pair -------------------------------------------------
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)
@@ -409,15 +428,9 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
 {
     constexpr int N = N1 * N2;
     // forward along rows (centring the tile on the way in): lanes take consecutive rows
-    for (int t = tid; t < rows_in * N2; t += nt) {
-        const int y = t % rows_in, n2 = t / rows_in;
-        fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre);
-    }
+    row_tasks(rows_in, N2, tid, nt, [&](int y, int n2) { fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre); });
     sync();
-    for (int t = tid; t < rows_in * N1; t += nt) {
-        const int y = t % rows_in, k1 = t / rows_in;
-        step_b<N1, N2, -1>(Z + y * RS, 1, k1);
-    }
+    row_tasks(rows_in, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, -1>(Z + y * RS, 1, k1); });
     sync();
     // forward along columns: lanes take consecutive columns
     for (int t = tid; t < N * N2; t += nt) {
@@ -456,16 +469,12 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
     }
     sync();
     // inverse along the rows that hold placements
-    for (int t = tid; t < rows_out * N1; t += nt) {
-        const int y = t % rows_out, k1 = t / rows_out;
-        step_b<N1, N2, 1>(Z + y * RS, 1, k1);
-    }
+    row_tasks(rows_out, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, 1>(Z + y * RS, 1, k1); });
     sync();
     // the last step hands its outputs to store(u, v, value) instead of writing them back
-    for (int t = tid; t < rows_out * N2; t += nt) {
-        const int y = t % rows_out, n2 = t / rows_out;
+    row_tasks(rows_out, N2, tid, nt, [&](int y, int n2) {
         inv_a_store<N1, N2>(Z + y * RS, 1, n2, tw, [&](int n, float2 v) { store(y, n, v); });
-    }
+    });
     sync();
 }
 
