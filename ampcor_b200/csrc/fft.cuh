@@ -261,25 +261,22 @@ HD void fwd_a(float2* base, int es, int n2, const float2* tw)
 }
 
 // Centring applied on the way in (the first pass over the rows): element n of row y gets sx
-// taken off its real part when y < wx and n < wx, and syh then syl off its imaginary part when
-// y < wy and n < wy.  Zero shifts leave the tile as it is.
+// taken off its real part when y < wx and n < wx.  A zero shift leaves the tile as it is.
 struct Centre {
     float sx;
     int wx;
-    float syh, syl;
-    int wy;
 };
 
 template <int N1, int N2>
 HD void fwd_a_centred(float2* row, int y, int n2, const float2* tw, const Centre& c)
 {
+    const int lim = y < c.wx ? c.wx : 0;
     float2 a[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
         const int n = N2 * n1 + n2;
         float2 v = row[n];
-        if (y < c.wx && n < c.wx) v.x -= c.sx;
-        if (y < c.wy && n < c.wy) v.y = (v.y - c.syh) - c.syl;
+        if (n < lim) v.x -= c.sx;
         a[n1] = v;
     }
     Dft<N1, -1>::run(a);

@@ -106,14 +106,6 @@ __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
     return var > 0.0f ? __frsqrt_rn(var) : 0.0f;
 }
 
-// error-free sum of two floats (Knuth's two-sum): hi + lo == a + b exactly
-__device__ __forceinline__ void two_sum(float a, float b, float& hi, float& lo)
-{
-    hi = a + b;
-    const float bb = hi - a;
-    lo = (a - (hi - bb)) + (b - bb);
-}
-
 // 1/sigma_box of every placement from the window in the tile's real parts (rows RS apart), the
 // values shifted by sx (the window mean: the box variance does not change and the column sums
 // keep their digits).  sigma^2 = S2 - S1^2 / R^2 over the R x R box, its sum of squared deviations
@@ -124,12 +116,12 @@ __device__ __forceinline__ void two_sum(float a, float b, float& hi, float& lo)
 // of the first placement's rows (FP32 runs of 8 rows added in FP64) and the slides
 // delta(i) = t(i + R) - t(i) of its share of the placement rows (FP32: a slide is small next to a
 // column sum); after one exchange (part, FP64) each thread starts its share at V(0) plus the
-// earlier shares' slides, carries the running sums as float pairs (two-sum, no rounding) and
+// earlier shares' slides (as a float pair) and adds the FP32 sum of its own slides so far, and
 // writes V(u, x) of its rows as floats into the slots (V1 at slot u W + x, V2 at C W + u W + x).
 // Then one warp per placement row (two rows at a time) forms the box sums
 // S(v) = sum_{x in [v, v + R)} V(x): S(0) as an FP64 warp sum, the others as S(0) plus an FP32 scan
-// of V(v + R) - V(v) across the lanes.  Conversions between float and double are few: they run
-// at a fraction of the FP32 rate.  Ends with a barrier.
+// of V(v + R) - V(v) across the lanes.  The phases are bound by instruction issue, so the FP64
+// work and the float-double conversions are kept to a few per column.  Ends with a barrier.
 __device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float sx, StatSlots vs,
                                double* part, float* invs)
 {
@@ -155,9 +147,10 @@ __device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float
         }
         float e1 = 0.0f, e2 = 0.0f;
         for (int i = s * D / nseg, i1 = (s + 1) * D / nseg; i < i1; ++i) {
-            const float a = tv(i + R), b = tv(i);
-            e1 += a - b;
-            e2 = fmaf(a - b, a + b, e2);
+            const float a = Z[(i + R) * RS + x].x, b = Z[i * RS + x].x;
+            const float d = a - b;
+            e1 += d;
+            e2 = fmaf(d, (a + b) - 2.0f * sx, e2);
         }
         part[(0 * nseg + s) * W + x] = b1;
         part[(1 * nseg + s) * W + x] = b2;
@@ -175,8 +168,11 @@ __device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float
             v1 += part[(2 * nseg + q) * W + x];
             v2 += part[(3 * nseg + q) * W + x];
         }
-        float h1 = (float)v1, l1 = (float)(v1 - (double)h1);
-        float h2 = (float)v2, l2 = (float)(v2 - (double)h2);
+        // V(u) = V(start) + P(u), P the FP32 sum of this share's slides so far (small next to
+        // V); V(start) as a float pair
+        const float h1 = (float)v1, l1 = (float)(v1 - (double)h1);
+        const float h2 = (float)v2, l2 = (float)(v2 - (double)h2);
+        float p1 = 0.0f, p2 = 0.0f;
         const int i1 = (s + 1) * D / nseg;
         constexpr int kB = 4;  // window rows read ahead of the running sums
         for (int i0 = s * D / nseg; i0 < i1; i0 += kB) {
@@ -184,24 +180,22 @@ __device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float
 #pragma unroll
             for (int k = 0; k < kB; ++k) {
                 const int i = min(i0 + k, i1 - 1);
-                a[k] = tv(i + R);
-                b[k] = tv(i);
+                a[k] = Z[(i + R) * RS + x].x;
+                b[k] = Z[i * RS + x].x;
             }
 #pragma unroll
             for (int k = 0; k < kB; ++k)
                 if (i0 + k < i1) {
-                    *vs.at((i0 + k) * W + x) = h1 + l1;
-                    *vs.at((C + i0 + k) * W + x) = h2 + l2;
-                    float e;
-                    two_sum(h1, a[k] - b[k], h1, e);
-                    l1 += e;
-                    two_sum(h2, (a[k] - b[k]) * (a[k] + b[k]), h2, e);
-                    l2 += e;
+                    *vs.at((i0 + k) * W + x) = h1 + (l1 + p1);
+                    *vs.at((C + i0 + k) * W + x) = h2 + (l2 + p2);
+                    const float d = a[k] - b[k];
+                    p1 += d;
+                    p2 = fmaf(d, (a[k] + b[k]) - 2.0f * sx, p2);
                 }
         }
         if (s == nseg - 1) {
-            *vs.at(D * W + x) = h1 + l1;
-            *vs.at((C + D) * W + x) = h2 + l2;
+            *vs.at(D * W + x) = h1 + (l1 + p1);
+            *vs.at((C + D) * W + x) = h2 + (l2 + p2);
         }
     }
     __syncthreads();
@@ -386,10 +380,9 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     // One sweep of sums, combined across the block in FP64: the window's sum and sum of squares,
     // the chip's sum (compensated) and sum of squares, each thread over a few dozen samples in
     // FP32.  They give the chip mean, 1/|r'| with |r'|^2 = sum r^2 - R^2 mean^2 (refStats.cu:118-302)
-    // and |t'| of the centred window; the centring itself (window mean off the real parts, chip
-    // mean off the imaginary parts, the latter as two floats so that r' carries the FP64 mean)
-    // happens as the first transform pass reads the tile.  The window mean only conditions the
-    // transform and |t'| only scales its error bound.
+    // and |t'| of the centred window.  The chip mean comes off as the chip goes into the tile (two
+    // floats, so that r' carries the FP64 mean), the window mean as the first transform pass reads
+    // the tile; the latter only conditions the transform and |t'| only scales its error bound.
     double acc4[4];
     {
         float sw = 0.0f, sw2 = 0.0f, sc = 0.0f, cc = 0.0f, sc2 = 0.0f;
@@ -426,19 +419,20 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     const double st = fmax(acc4[3] - cells_w * mean_w * mean_w, 0.0);
     const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
     const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
-    const fft::Centre centre{(float)mean_w, W, mc_hi, mc_lo, R};
+    const fft::Centre centre{(float)mean_w, W};
     if (!inv_b) {
         double* part = reinterpret_cast<double*>(ssm + g.off_gam);
         const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
         spec_box_stats(Z, RS, g, centre.sx, vs, part, invs);
     }
-    // the chip into the imaginary parts, zeros around it
+    // the zero-mean chip into the imaginary parts (its FP64 mean off as two floats), zeros around
+    // it
 #pragma unroll
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
             const int y = warp + kWarps * j, x = lane + 32 * i;
-            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = cr[j][i];
+            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = y < R && x < R ? (cr[j][i] - mc_hi) - mc_lo : 0.0f;
         }
     __syncthreads();
 

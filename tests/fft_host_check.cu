@@ -60,13 +60,12 @@ double check2d(int W, int R, std::mt19937& g, bool centre_in_pass = false)
     for (auto v : t) mw += v;
     mw /= (double)W * W;
     for (int y = 0; y < W; ++y) for (int x = 0; x < W; ++x) Z[y * RS + x].x = t[y * W + x];
+    // the chip centred as the kernel does it (two float subtractions carrying the FP64 mean)
+    const float mhi = (float)mr, mlo = (float)(mr - (double)mhi);
     for (int y = 0; y < R; ++y)
-        for (int x = 0; x < R; ++x) Z[y * RS + x].y = centre_in_pass ? raw[y * R + x] : r[y * R + x];
-    Centre ctr{0.0f, 0, 0.0f, 0.0f, 0};
-    if (centre_in_pass) {
-        const float hi = (float)mr;
-        ctr = Centre{(float)mw, W, hi, (float)(mr - (double)hi), R};
-    }
+        for (int x = 0; x < R; ++x) Z[y * RS + x].y = centre_in_pass ? (raw[y * R + x] - mhi) - mlo : r[y * R + x];
+    Centre ctr{0.0f, 0};
+    if (centre_in_pass) ctr = Centre{(float)mw, W};
     std::vector<int> neg(N);
     for (int q = 0; q < N; ++q) neg[q] = neg_pos<N1, N2>(q);
     std::vector<float> num(C * N);
