@@ -122,8 +122,9 @@ __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
 // S(v) = sum_{x in [v, v + R)} V(x): S(0) as an FP64 warp sum, the others as S(0) plus an FP32 scan
 // of V(v + R) - V(v) across the lanes.  The phases are bound by instruction issue, so the FP64
 // work and the float-double conversions are kept to a few per column.  Ends with a barrier.
-__device__ void spec_box_stats(const float2* Z, int RS, const SpecGeom& g, float sx, StatSlots vs,
-                               double* part, float* invs)
+template <int RS>
+__device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, StatSlots vs, double* part,
+                               float* invs)
 {
     const int R = g.R, W = g.W, C = g.C, nseg = g.nseg, D = C - 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -330,7 +331,10 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         return;
     }
     constexpr int N = N1 * N2;
-    const int RS = g.RS, W = g.W, R = g.R, C = g.C;
+    // the tile's row stride is always N + 1 (odd); as a constant every element offset of a row or
+    // column walk is an immediate
+    constexpr int RS = N + 1;
+    const int W = g.W, R = g.R, C = g.C;
     float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
     float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
     int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
@@ -423,7 +427,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     if (!inv_b) {
         double* part = reinterpret_cast<double*>(ssm + g.off_gam);
         const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
-        spec_box_stats(Z, RS, g, centre.sx, vs, part, invs);
+        spec_box_stats<RS>(Z, g, centre.sx, vs, part, invs);
     }
     // the zero-mean chip into the imaginary parts (its FP64 mean off as two floats), zeros around
     // it

@@ -175,6 +175,13 @@ int main()
     e2 = fmax(e2, check2d<8, 16>(128, 64, g, true));
     e2 = fmax(e2, check2d<10, 16>(160, 128, g, true));
     e2 = fmax(e2, check2d<8, 12>(90, 60, g, true));
+    // odd first and second radices and short lengths
+    e2 = fmax(e2, check2d<5, 8>(40, 32, g, true));
+    e2 = fmax(e2, check2d<8, 15>(120, 96, g, true));
+    e2 = fmax(e2, check2d<4, 6>(24, 16, g, true));
+    e2 = fmax(e2, check2d<8, 10>(80, 64, g, true));
+    e2 = fmax(e2, check2d<4, 4>(16, 8, g, true));
+    e2 = fmax(e2, check2d<4, 8>(32, 20, g, true));
     double e3 = 0;
     e3 = fmax(e3, check_upsample<8, 8, 8, 16>(g));
     e3 = fmax(e3, check_upsample<8, 10, 10, 16>(g));
