@@ -380,6 +380,10 @@ std::vector<float> taps_table(int N, int f, int s0, int len)
 
 }  // namespace
 
+// bands of a host-buffer job of the spectral form: the rasters go up band by band while the pairs
+// whose tiles lie in the bands already up are correlated
+constexpr int kHostBands = 12;
+
 struct ampcor_handle {
     ampcor_params prm{};
     int R = 0, W = 0, C = 0, M = 0, E = 0, f = 0, m = 0, z = 0, Rf = 0, Wf = 0, Cf = 0, Z = 0;
@@ -388,6 +392,9 @@ struct ampcor_handle {
     ZoomGeom zg{};
     int refine_smem = 0;
     cudaStream_t stream = nullptr;
+    // host-buffer jobs: raster bands uploaded on their own stream, one event per band
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t band_ev[kHostBands + 1] = {};
     float* d_chip_taps = nullptr;
     float* d_win_taps = nullptr;
     float* d_zoom_taps = nullptr;
@@ -693,53 +700,94 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
 
 // spectral form: amplitudes of both rasters once, then per chunk: coarse statistics -> coarse
 // correlation (FFT) -> refinement -> fine statistics -> fine correlation (FFT) -> zoom
-int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
-                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+// the amplitude rasters of a spectral job and, where the windows tile a raster, its box statistics
+struct SpecRasters {
+    float* amp_ref = nullptr;
+    float* amp_tgt = nullptr;
+    bool shared = false;        // one raster holds chips and windows
+    bool raster_stats = false;  // coarse box statistics once per raster, else inside the kernel
+    long long rows = 0;         // box rows of the secondary raster (tgt_lines - R + 1)
+    size_t cells = 0;           // rows * stride
+    InvSource inv_c{nullptr, nullptr, 0};
+};
+
+// buffers of a spectral job of `pairs` pairs; no launches
+int spec_rasters(ampcor_handle* h, const PairSource& src, long long pairs, SpecRasters& r)
 {
-    if (pairs == 0) return AMPCOR_OK;
     int rc = ensure_refined(h);
     if (rc) return rc;
     if ((rc = ensure_fine_out(h, (size_t)pairs))) return rc;
-    const bool shared = src.ref_base == src.tgt_base;
-    const size_t need = (size_t)src.ref_count + (shared ? 0 : (size_t)src.tgt_count);
-    if ((rc = grow(h, h->d_amp, h->amp_cap, need, "amplitude rasters"))) return rc;
-    float* amp_ref = h->d_amp;
-    float* amp_tgt = shared ? h->d_amp : h->d_amp + src.ref_count;
+    r.shared = src.ref_base == src.tgt_base;
+    const size_t need = (size_t)src.ref_count + (r.shared ? 0 : (size_t)src.tgt_count);
+    // 16 floats of slack here and below: staged copies round rows out to 16-byte boundaries
+    if ((rc = grow(h, h->d_amp, h->amp_cap, need + 16, "amplitude rasters"))) return rc;
+    r.amp_ref = h->d_amp;
+    r.amp_tgt = r.shared ? h->d_amp : h->d_amp + src.ref_count;
+    // coarse box statistics once per raster where the windows tile a raster (they overlap), else
+    // inside the correlation kernel from the window it holds (as for every fine window)
+    r.rows = src.tgt_lines - h->R + 1;
+    r.raster_stats = src.tgt_lines > 0 && r.rows > 0 && src.tgt_stride <= 12288;
+    r.inv_c = InvSource{nullptr, nullptr, 0};
+    if (r.raster_stats) {
+        r.cells = (size_t)r.rows * (size_t)src.tgt_stride;
+        if ((rc = grow(h, h->d_vsum, h->vsum_cap, 2 * r.cells, "box statistics")) ||
+            (rc = grow(h, h->d_inv_raster, h->inv_raster_cap, r.cells + 16, "box statistics")))
+            return rc;
+        r.inv_c = InvSource{h->d_inv_raster, src.tgt_off, src.tgt_stride};
+    }
+    return AMPCOR_OK;
+}
+
+// amplitudes of samples [ref_lo, ref_hi) of the reference source and [tgt_lo, tgt_hi) of the
+// secondary, box statistics of box rows [box_lo, box_hi); a band gives the same values as the
+// whole raster
+int spec_band(ampcor_handle* h, const PairSource& src, const SpecRasters& r, long long ref_lo,
+              long long ref_hi, long long tgt_lo, long long tgt_hi, long long box_lo, long long box_hi,
+              cudaStream_t st)
+{
     auto detect = [&](const float2* x, long long n, float* y) {
         const long long blocks = std::min<long long>((n + 1023) / 1024, 148 * 16);
         if (n > 0) detect_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, st>>>(x, n, y);
+        return n > 0 ? 1 : 0;
     };
     cudaEvent_t a0 = mark(h, st);
-    detect(src.ref_base, src.ref_count, amp_ref);
-    if (!shared) detect(src.tgt_base, src.tgt_count, amp_tgt);
-    CK(h, cudaGetLastError(), "launching the detection kernel");
-    // coarse box statistics once per raster where the windows tile a raster (they overlap), else
-    // inside the correlation kernel from the window it holds (as for every fine window)
-    InvSource inv_c{nullptr, nullptr, 0};
-    const long long rows = src.tgt_lines - h->R + 1;
-    const bool raster_stats = src.tgt_lines > 0 && rows > 0 && src.tgt_stride <= 12288;
-    if (raster_stats) {
-        const size_t cells = (size_t)rows * (size_t)src.tgt_stride;
-        if ((rc = grow(h, h->d_vsum, h->vsum_cap, 2 * cells, "box statistics")) ||
-            (rc = grow(h, h->d_inv_raster, h->inv_raster_cap, cells, "box statistics")))
-            return rc;
-        const dim3 vg((unsigned)((src.tgt_stride + 255) / 256), (unsigned)((rows + kVBlock - 1) / kVBlock));
-        box_vsum_kernel<<<vg, 256, 0, st>>>(amp_tgt, src.tgt_lines, src.tgt_stride, h->R, h->d_vsum,
-                                            h->d_vsum + cells);
-        const int psmem = (int)((2 * (src.tgt_stride + 1) + 2 * kWarps) * sizeof(double));
-        box_inv_kernel<<<(unsigned)rows, kThreads, psmem, st>>>(h->d_vsum, h->d_vsum + cells, rows,
-                                                               src.tgt_stride, h->R, h->d_inv_raster);
-        CK(h, cudaGetLastError(), "launching the box statistics kernels");
-        inv_c = InvSource{h->d_inv_raster, src.tgt_off, src.tgt_stride};
+    int kernels = 0;
+    if (r.shared) {
+        const long long lo = std::min(ref_lo, tgt_lo), hi = std::max(ref_hi, tgt_hi);
+        kernels += detect(src.ref_base + lo, hi - lo, r.amp_ref + lo);
+    } else {
+        kernels += detect(src.ref_base + ref_lo, ref_hi - ref_lo, r.amp_ref + ref_lo);
+        kernels += detect(src.tgt_base + tgt_lo, tgt_hi - tgt_lo, r.amp_tgt + tgt_lo);
     }
-    keep(h, 3, a0, mark(h, st), (shared ? 1 : 2) + (raster_stats ? 2 : 0));
-    const SpecSource cs{amp_ref, src.ref_stride, src.ref_off, 0, amp_tgt, src.tgt_stride, src.tgt_off, 0};
+    CK(h, cudaGetLastError(), "launching the detection kernel");
+    if (r.raster_stats && box_hi > box_lo) {
+        const long long vlo = box_lo / kVBlock * kVBlock;
+        const dim3 vg((unsigned)((src.tgt_stride + 255) / 256), (unsigned)((box_hi - vlo + kVBlock - 1) / kVBlock));
+        box_vsum_kernel<<<vg, 256, 0, st>>>(r.amp_tgt, src.tgt_stride, h->R, vlo, box_hi, h->d_vsum,
+                                            h->d_vsum + r.cells);
+        const int psmem = (int)((2 * (src.tgt_stride + 1) + 2 * kWarps) * sizeof(double));
+        box_inv_kernel<<<(unsigned)(box_hi - box_lo), kThreads, psmem, st>>>(
+            h->d_vsum, h->d_vsum + r.cells, box_lo, box_hi, src.tgt_stride, h->R, h->d_inv_raster);
+        CK(h, cudaGetLastError(), "launching the box statistics kernels");
+        kernels += 2;
+    }
+    keep(h, 3, a0, mark(h, st), kernels);
+    return AMPCOR_OK;
+}
+
+// the correlation pipeline of pairs [p0, p1), chunk by chunk
+int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, long long p0, long long p1,
+               float2* offsets, PairDiag* diag, float* coarse_surfaces, float* refined_surfaces,
+               cudaStream_t st)
+{
+    int rc = AMPCOR_OK;
+    const SpecSource cs{r.amp_ref, src.ref_stride, src.ref_off, 0, r.amp_tgt, src.tgt_stride, src.tgt_off, 0};
     const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
-    for (long long c0 = 0; c0 < pairs; c0 += (long long)h->chunk) {
-        const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, pairs - c0);
+    for (long long c0 = p0; c0 < p1; c0 += (long long)h->chunk) {
+        const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, p1 - c0);
         cudaEvent_t b = mark(h, st);
-        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, inv_c,
+        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
                           reinterpret_cast<const float2*>(h->d_tw_c),
                           SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
            "launching the spectral coarse correlation");
@@ -772,6 +820,18 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
         keep(h, 5, f, mark(h, st));
     }
     return AMPCOR_OK;
+}
+
+int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
+                 PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
+{
+    if (pairs == 0) return AMPCOR_OK;
+    SpecRasters r;
+    int rc = spec_rasters(h, src, pairs, r);
+    if (rc) return rc;
+    if ((rc = spec_band(h, src, r, 0, src.ref_count, 0, src.tgt_count, 0, r.raster_stats ? r.rows : 0, st)))
+        return rc;
+    return spec_pairs(h, src, r, 0, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
 }
 
 int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
@@ -993,6 +1053,9 @@ int ampcor_destroy(ampcor_handle* h)
     drop_marks(h);
     if (h->h_arena) cudaFreeHost(h->h_arena);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
+    for (cudaEvent_t e : h->band_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return AMPCOR_OK;
@@ -1132,6 +1195,85 @@ int ampcor_synchronize(ampcor_handle* h, void* stream)
     return AMPCOR_OK;
 }
 
+// A host-buffer job of the spectral form in kHostBands groups of consecutive pairs: group g needs
+// the raster rows up to the deepest chip and window of pairs 0 .. end of g (so pairs in raster
+// order need about a band each); those rows go up on the copy stream while the compute stream
+// correlates group g - 1, then the compute stream detects the new rows, extends the box
+// statistics to the box rows they complete and correlates group g.  Same kernels and the same
+// values as one upload followed by the whole job; the upload hides behind all but the first band.
+int correlate_host_banded(ampcor_handle* h, const ampcor_job* j)
+{
+    int rc = AMPCOR_OK;
+    cudaStream_t st = h->stream;
+    if (!h->copy_stream)
+        CK(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "creating the upload stream");
+    for (cudaEvent_t& e : h->band_ev)
+        if (!e) CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating the band events");
+    if ((rc = ensure_pairs(h, j->pairs))) return rc;
+    const long long P = (long long)j->pairs;
+    const long long rs = j->ref_samples, ts = j->tgt_samples;
+    const long long rlines = j->ref_lines, tlines = j->tgt_lines;
+    // the raster buffers may still be read by the previous job's kernels
+    CK(h, cudaEventRecord(h->band_ev[kHostBands], st), "ordering the upload");
+    CK(h, cudaStreamWaitEvent(h->copy_stream, h->band_ev[kHostBands], 0), "ordering the upload");
+    CK(h, cudaMemcpyAsync(h->d_ulhc, j->ulhc, 4 * P * sizeof(int32_t), cudaMemcpyHostToDevice, st),
+       "uploading the pair corners");
+    pair_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(h->d_ulhc, P, rlines, rs, tlines, ts, h->R,
+                                                                      h->W, h->d_ref_off, h->d_tgt_off, h->d_bad);
+    CK(h, cudaGetLastError(), "launching the pair offsets kernel");
+    const float2* dref = reinterpret_cast<const float2*>(h->d_ref_raster);
+    const float2* dtgt = reinterpret_cast<const float2*>(h->d_tgt_raster);
+    PairSource src{dref, h->d_ref_off, rs, dtgt, h->d_tgt_off, ts, rlines * rs, tlines * ts, tlines};
+    SpecRasters r;
+    if ((rc = spec_rasters(h, src, P, r))) return rc;
+    const float2* href = static_cast<const float2*>(j->ref);
+    const float2* htgt = static_cast<const float2*>(j->tgt);
+    // group ends on whole waves of the correlation kernels (two CTAs per SM at most) once a job
+    // has a few waves per group
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long granule = std::min<long long>(2LL * std::max(sms, 1), std::max<long long>(1, P / (4 * kHostBands)));
+    long long up_r = 0, up_t = 0, boxes = 0, need_r = 0, need_t = 0, p0 = 0;
+    for (int g = 0; g < kHostBands && p0 < P; ++g) {
+        long long p1 = (P * (g + 1) / kHostBands + granule / 2) / granule * granule;
+        if (g + 1 == kHostBands || p1 > P) p1 = P;
+        if (p1 <= p0) continue;
+        for (long long p = p0; p < p1; ++p) {
+            need_r = std::max<long long>(need_r, std::min<long long>((long long)j->ulhc[4 * p] + h->R, rlines));
+            need_t = std::max<long long>(need_t, std::min<long long>((long long)j->ulhc[4 * p + 2] + h->W, tlines));
+        }
+        const long long nr = p1 == P ? rlines : std::max(need_r, up_r);
+        const long long nt = p1 == P ? tlines : std::max(need_t, up_t);
+        if (nr > up_r)
+            CK(h, cudaMemcpyAsync(static_cast<float2*>(h->d_ref_raster) + up_r * rs, href + up_r * rs, (nr - up_r) * rs * sizeof(float2),
+                                  cudaMemcpyHostToDevice, h->copy_stream),
+               "uploading the reference raster");
+        if (nt > up_t)
+            CK(h, cudaMemcpyAsync(static_cast<float2*>(h->d_tgt_raster) + up_t * ts, htgt + up_t * ts, (nt - up_t) * ts * sizeof(float2),
+                                  cudaMemcpyHostToDevice, h->copy_stream),
+               "uploading the secondary raster");
+        CK(h, cudaEventRecord(h->band_ev[g], h->copy_stream), "recording a band");
+        CK(h, cudaStreamWaitEvent(st, h->band_ev[g], 0), "waiting for a band");
+        const long long nb = r.raster_stats ? std::max<long long>(0, std::min(r.rows, nt - h->R + 1)) : 0;
+        if ((rc = spec_band(h, src, r, up_r * rs, nr * rs, up_t * ts, nt * ts, boxes, std::max(boxes, nb), st)))
+            return rc;
+        boxes = std::max(boxes, nb);
+        up_r = nr;
+        up_t = nt;
+        if ((rc = spec_pairs(h, src, r, p0, p1, reinterpret_cast<float2*>(h->d_job_offsets),
+                             j->diag ? reinterpret_cast<PairDiag*>(h->d_job_diag) : nullptr, nullptr, nullptr, st)))
+            return rc;
+        p0 = p1;
+    }
+    CK(h, cudaMemcpyAsync(j->offsets, h->d_job_offsets, 2 * P * sizeof(float), cudaMemcpyDeviceToHost, st),
+       "downloading the offsets");
+    if (j->diag)
+        CK(h, cudaMemcpyAsync(j->diag, h->d_job_diag, P * sizeof(ampcor_pair_diag), cudaMemcpyDeviceToHost, st),
+           "downloading the diagnostics");
+    return AMPCOR_OK;
+}
+
 int ampcor_correlate_host(ampcor_handle* h, const ampcor_job* j)
 {
     int rc = check_job(h, j);
@@ -1158,6 +1300,11 @@ int ampcor_correlate_host(ampcor_handle* h, const ampcor_job* j)
     if ((rc = grow(h, h->d_job_offsets, h->job_offsets_cap, 2 * j->pairs, "offsets"))) return rc;
     if (j->diag && (rc = grow(h, h->d_job_diag, h->job_diag_cap, j->pairs, "diagnostics"))) return rc;
     cudaStream_t st = h->stream;
+    if (h->form == kFormSpectral && j->pairs >= 2 * kHostBands && !j->coarse_surfaces && !j->refined_surfaces &&
+        j->ref != j->tgt) {
+        if ((rc = correlate_host_banded(h, j))) return rc;
+        return ampcor_synchronize(h, st);
+    }
     CK(h, cudaMemcpyAsync(h->d_ref_raster, j->ref, rb, cudaMemcpyHostToDevice, st), "uploading the reference raster");
     CK(h, cudaMemcpyAsync(h->d_tgt_raster, j->tgt, tb, cudaMemcpyHostToDevice, st), "uploading the secondary raster");
     CK(h, cudaMemcpyAsync(h->d_ulhc, j->ulhc, 4 * j->pairs * sizeof(int32_t), cudaMemcpyHostToDevice, st),

@@ -245,14 +245,16 @@ struct SpecOut {
 
 // |z| of every sample of a complex array (n samples)
 __global__ void detect_kernel(const float2* src, long long n, float* dst);
-// FP64 box statistics of a whole amplitude raster, for windows that overlap (the coarse stage of a
-// raster job): column sums over R rows (v1: sum a, v2: sum a^2; rows = lines - R + 1 of them),
-// then per row prefix sums and 1/sqrt(var) of the R x R box at every (y, x), x <= samples - R
+// FP64 box statistics of an amplitude raster, for windows that overlap (the coarse stage of a
+// raster job): column sums over R rows (v1: sum a, v2: sum a^2) for box rows [row_lo, row_hi)
+// (box row y covers raster rows y .. y + R - 1; row_lo a multiple of kVBlock, so that a band
+// computes its rows exactly as the whole raster would), then per box row prefix sums and
+// 1/sqrt(var) of the R x R box at every (y, x), x <= samples - R
 constexpr int kVBlock = 64;  // rows slid per thread of the column sums
-__global__ void box_vsum_kernel(const float* a, long long lines, long long samples, int R, double* v1,
-                                double* v2);
-__global__ void box_inv_kernel(const double* v1, const double* v2, long long rows, long long samples,
-                               int R, float* inv);
+__global__ void box_vsum_kernel(const float* a, long long samples, int R, long long row_lo,
+                                long long row_hi, double* v1, double* v2);
+__global__ void box_inv_kernel(const double* v1, const double* v2, long long row_lo, long long row_hi,
+                               long long samples, int R, float* inv);
 
 // where a spectral correlation finds 1/sigma_box of placement (u, v) of chunk-local pair b:
 // base + off[pair0 + b] + u stride + v when off is given, else base + b C^2 + u C + v

@@ -632,14 +632,13 @@ __global__ void detect_kernel(const float2* __restrict__ src, long long n, float
 }
 
 __global__ void __launch_bounds__(256)
-box_vsum_kernel(const float* __restrict__ a, long long lines, long long samples, int R,
-                double* __restrict__ v1, double* __restrict__ v2)
+box_vsum_kernel(const float* __restrict__ a, long long samples, int R, long long row_lo,
+                long long row_hi, double* __restrict__ v1, double* __restrict__ v2)
 {
     const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long rows = lines - R + 1;
-    const long long y0 = (long long)blockIdx.y * kVBlock;
-    if (x >= samples || y0 >= rows) return;
-    const long long y1 = y0 + kVBlock < rows ? y0 + kVBlock : rows;
+    const long long y0 = row_lo + (long long)blockIdx.y * kVBlock;
+    if (x >= samples || y0 >= row_hi) return;
+    const long long y1 = y0 + kVBlock < row_hi ? y0 + kVBlock : row_hi;
     const float* col = a + x;
     double a1[4] = {0.0, 0.0, 0.0, 0.0}, a2[4] = {0.0, 0.0, 0.0, 0.0};
     int i = 0;
@@ -672,12 +671,12 @@ box_vsum_kernel(const float* __restrict__ a, long long lines, long long samples,
 // one CTA per box row: FP64 exclusive prefix sums of the row's column sums (in chunks of eight per
 // thread, a fixed order), then the box of every x from two prefix differences
 __global__ void __launch_bounds__(kThreads)
-box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, long long rows,
-               long long samples, int R, float* __restrict__ inv)
+box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, long long row_lo,
+               long long row_hi, long long samples, int R, float* __restrict__ inv)
 {
     extern __shared__ __align__(16) double psm[];
-    const long long y = blockIdx.x;
-    if (y >= rows) return;
+    const long long y = row_lo + blockIdx.x;
+    if (y >= row_hi) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* P1 = psm;
     double* P2 = psm + samples + 1;

@@ -134,7 +134,10 @@ int ampcor_synchronize(ampcor_handle* handle, void* stream);
 
 /* Same as ampcor_correlate but every pointer of job is host memory: the call uploads the
    rasters and corners, runs the batch and copies the offsets (and optional outputs) back before
-   it returns.  This is the end-to-end path of pkg/ampcor/correlators/CUDA.py:22-61. */
+   it returns.  This is the end-to-end path of pkg/ampcor/correlators/CUDA.py:22-61.  In the
+   spectral form the rasters go up in bands of rows while the pairs whose tiles are already up
+   are correlated (same offsets as one upload first); with page-locked host rasters the upload
+   then hides behind the correlation, with pageable ones it does not. */
 int ampcor_correlate_host(ampcor_handle* handle, const ampcor_job* job);
 
 /* Placements per axis of the coarse (C = W - R + 1) and refined (Cf = 2 f m + 1) surfaces and

@@ -179,6 +179,21 @@ def test_host_path_matches_device_path():
     assert np.array_equal(diag, dev["diag"])
 
 
+@pytest.mark.parametrize("order", ["reversed", "shuffled"])
+def test_host_path_bands_any_pair_order(order):
+    # host-buffer jobs upload the rasters in bands and correlate the pairs whose tiles are up;
+    # pairs out of raster order only delay the bands, the offsets stay those of the device path
+    w = synth.plain_512()
+    perm = np.arange(w.pairs)[::-1] if order == "reversed" else np.random.default_rng(5).permutation(w.pairs)
+    ulhc = np.ascontiguousarray(w.ulhc[perm])
+    worker = Worker(pairs=w.pairs, chip=(32, 32), window=(48, 48), refine_factor=2,
+                    refine_margin=4, zoom_factor=4)
+    off, diag = worker.correlate(w.ref, w.tgt, ulhc, diag=True)
+    dev = run_device(w, form=worker.form)
+    assert np.array_equal(off, dev["offsets"][perm])
+    assert np.array_equal(diag, dev["diag"][perm])
+
+
 def test_extension_mirror_matches_raster_path():
     # the reference's call sequence (pkg/ampcor/correlators/CUDA.py:45-58)
     w = synth.plain_512()
