@@ -398,17 +398,20 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
                 sw2 = fmaf(t, t, sw2);
             }
         }
+        // register slots past the chip hold zeros in every lane: skipped (warp-uniform tests)
 #pragma unroll
         for (int j = 0; j < JN; ++j)
+            if (warp + kWarps * j < R)
 #pragma unroll
-            for (int i = 0; i < IN; ++i) {
-                const float r = cr[j][i];
-                const float yk = r - cc;
-                const float tk = sc + yk;
-                cc = (tk - sc) - yk;
-                sc = tk;
-                sc2 = fmaf(r, r, sc2);
-            }
+                for (int i = 0; i < IN; ++i)
+                    if (32 * i < R) {
+                        const float r = cr[j][i];
+                        const float yk = r - cc;
+                        const float tk = sc + yk;
+                        cc = (tk - sc) - yk;
+                        sc = tk;
+                        sc2 = fmaf(r, r, sc2);
+                    }
         acc4[0] = (double)sc - (double)cc;
         acc4[1] = sc2;
         acc4[2] = sw;
