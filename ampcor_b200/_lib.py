@@ -24,6 +24,7 @@ E_BOUNDS = 5
 E_STATE = 6
 FLAG_REF_COMPAT = 1
 FLAG_PLAIN_FP32 = 2
+FLAG_DERAMP = 4
 
 STATUS_NAMES = {
     OK: "AMPCOR_OK",

@@ -609,7 +609,7 @@ int run_plain(ampcor_handle* h, const PairSource& src, long long pairs, float2* 
         a = mark(h, st);
         refine_kernel<<<(unsigned)n, kThreads, h->refine_smem, st>>>(
             src, c0, n, h->d_coarse, h->ic, h->iw, h->d_chip_taps, h->d_win_taps, h->d_refined,
-            h->refined_stride);
+            h->refined_stride, (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0);
         CK(h, cudaGetLastError(), "launching the refinement kernel");
         cudaEvent_t b = mark(h, st);
         keep(h, 1, a, b);
@@ -680,7 +680,7 @@ int run_tensor(ampcor_handle* h, const PairSource& src, long long pairs, float2*
         keep(h, 0, b, c);
         refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
                                                            h->d_chip_taps, h->d_win_taps,
-                                                           h->d_refined, h->refined_stride);
+                                                           h->d_refined, h->refined_stride, (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0);
         cudaEvent_t d = mark(h, st);
         keep(h, 1, c, d);
         window_stats_real_kernel<<<n, kThreads, h->gsf.smem_bytes, st>>>(rt, n, h->gsf, h->d_inv_f);
@@ -796,16 +796,17 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
         if (h->refine_fft) {
             const float2* tw = reinterpret_cast<const float2*>(h->d_tw_refine);
             CK(h, launch_spec_refine(h->R, n, st, src.ref_base, src.ref_off, src.ref_stride, nullptr, c0,
-                                     n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0),
+                                     n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0,
+                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0),
                "launching the chip refinement");
             CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
                                      c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
-                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf),
+                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf, (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0),
                "launching the window refinement");
         } else {
             refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
                                                                h->d_chip_taps, h->d_win_taps,
-                                                               h->d_refined, h->refined_stride);
+                                                               h->d_refined, h->refined_stride, (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0);
             CK(h, cudaGetLastError(), "launching the refinement kernel");
         }
         cudaEvent_t e = mark(h, st);
@@ -1616,7 +1617,8 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
     for (long long c0 = 0; c0 < P; c0 += chunk) {
         const long long n = std::min(chunk, P - c0);
         refine_kernel<<<(unsigned)n, kThreads, refine_smem, st>>>(src, c0, n, coarse, ic, iw, taps,
-                                                                  taps + chip_taps, refined, refined_stride);
+                                                                  taps + chip_taps, refined, refined_stride,
+                                                                  (p->flags & AMPCOR_FLAG_DERAMP) ? 1 : 0);
         fine_kernel<<<(unsigned)n, kThreads, gf.smem_bytes, st>>>(
             refined, refined_stride, c0, n, ref_off, gf, zg, taps + chip_taps + win_taps, coarse, peak, M, f,
             m, (p->flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0, reinterpret_cast<float2*>(j->offsets),

@@ -242,7 +242,7 @@ __device__ __forceinline__ void interp_ring(const float* __restrict__ tp,
 // upsample the complex N x N tile at src by f and write the amplitudes (F x F, dense) to out
 __device__ void interp_tile(const float2* __restrict__ src, long long src_stride,
                             const InterpGeom& ig, const float* __restrict__ taps_g, float* smem,
-                            float* __restrict__ out)
+                            float* __restrict__ out, int deramp)
 {
     float2* X = reinterpret_cast<float2*>(smem + ig.off_x);
     float2* Y = reinterpret_cast<float2*>(smem + ig.off_y);
@@ -257,6 +257,8 @@ __device__ void interp_tile(const float2* __restrict__ src, long long src_stride
         X[r * NS + c] = __ldg(src + r * src_stride + c);
     }
     __syncthreads();
+    // the row-interpolated buffer is free until the rows are written: the deramp's scratch
+    if (deramp) deramp_tile(X, NS, N, reinterpret_cast<double*>(Y));
 
     // rows: Y[e][f q] = X[e][q], Y[e][f q + s] interpolated
     for (int idx = threadIdx.x; idx < N * N; idx += kThreads) {
@@ -477,7 +479,7 @@ coarse_kernel(PairSource src, long long pair0, long long pairs, NccGeom g, int m
 __global__ void __launch_bounds__(kThreads, 1)
 refine_kernel(PairSource src, long long pair0, long long pairs, const CoarseOut* coarse,
               InterpGeom chip_g, InterpGeom win_g, const float* chip_taps, const float* win_taps,
-              float* refined, long long refined_stride)
+              float* refined, long long refined_stride, int deramp)
 {
     extern __shared__ __align__(16) float smem[];
     if (blockIdx.x >= pairs) return;
@@ -485,10 +487,10 @@ refine_kernel(PairSource src, long long pair0, long long pairs, const CoarseOut*
     const long long roff = src.ref_off[p], toff = src.tgt_off[p];
     if (roff < 0 || toff < 0) return;
     float* out = refined + (long long)blockIdx.x * refined_stride;
-    interp_tile(src.ref_base + roff, src.ref_stride, chip_g, chip_taps, smem, out);
+    interp_tile(src.ref_base + roff, src.ref_stride, chip_g, chip_taps, smem, out, deramp);
     const CoarseOut co = coarse[p];
     interp_tile(src.tgt_base + toff + co.top * src.tgt_stride + co.left, src.tgt_stride, win_g,
-                win_taps, smem, out + (long long)chip_g.F * chip_g.F);
+                win_taps, smem, out + (long long)chip_g.F * chip_g.F, deramp);
 }
 
 __global__ void __launch_bounds__(kThreads, 1)

@@ -147,7 +147,7 @@ __global__ void coarse_kernel(PairSource src, long long pair0, long long pairs, 
 __global__ void refine_kernel(PairSource src, long long pair0, long long pairs,
                               const CoarseOut* coarse, InterpGeom chip_g, InterpGeom win_g,
                               const float* chip_taps, const float* win_taps, float* refined,
-                              long long refined_stride);
+                              long long refined_stride, int deramp);
 
 __global__ void fine_kernel(const float* refined, long long refined_stride, long long pair0,
                             long long pairs, const long long* ref_off, NccGeom g, ZoomGeom zg,
@@ -275,7 +275,7 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
-                               long long refined_stride, long long out_off);
+                               long long refined_stride, long long out_off, int deramp);
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
                         long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out);

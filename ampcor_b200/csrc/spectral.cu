@@ -499,7 +499,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 template <int N1, int N2, int F1, int F2, int CB>
 __device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
                              const float2* __restrict__ twn_g, const float2* __restrict__ twf_g,
-                             float* __restrict__ out)
+                             float* __restrict__ out, int deramp)
 {
     constexpr int N = N1 * N2, F = F1 * F2;
     constexpr int RSN = N + 1, RSF = F + 1, CBS = CB + 1;
@@ -515,6 +515,8 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     for (int k = tid; k < F; k += kThreads) twf[k] = __ldg(twf_g + k);
     cp_async_wait_all();
     __syncthreads();
+    // the upsampled-rows buffer is free until the rows are written: the deramp's scratch
+    if (deramp) deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
     // rows: forward N
     for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % N) * RSN, 1, t / N, twn);
     __syncthreads();
@@ -574,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, UpsampleGeom<N1, N2, F1, F2>::smem <
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
-                   long long out_off)
+                   long long out_off, int deramp)
 {
     extern __shared__ __align__(16) unsigned char rsm[];
     if (blockIdx.x >= pairs) return;
@@ -586,7 +588,7 @@ spec_refine_kernel(const float2* base, const long long* off, long long stride,
         src += co.top * stride + co.left;
     }
     fft_upsample<N1, N2, F1, F2, UpsampleGeom<N1, N2, F1, F2>::CB>(
-        src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off);
+        src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off, deramp);
 }
 
 // refinement (N, F = 2 N) pairs that are compiled: N, N1, N2, F1, F2
@@ -790,13 +792,13 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
-                               long long refined_stride, long long out_off)
+                               long long refined_stride, long long out_off, int deramp)
 {
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                     \
     if (n == NN) {                                                                             \
         spec_refine_kernel<A, B, C, D><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
             base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride,  \
-            out_off);                                                                          \
+            out_off, deramp);                                                                  \
         return cudaGetLastError();                                                             \
     }
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)

@@ -178,4 +178,53 @@ __device__ __forceinline__ void window_stats(const float* win, const NccGeom& g,
 }
 
 }  // namespace
+
+// Removes the linear phase ramp of an n x n complex tile in shared memory (rows `stride` samples
+// apart) before it is interpolated: phi_s = arg sum z(y, x + 1) conj z(y, x) and
+// phi_l = arg sum z(y + 1, x) conj z(y, x) (lag-one autocorrelations along samples and lines,
+// whose phases are the ramp's steps), then z(y, x) *= exp(-i (phi_s x + phi_l y)).  A Doppler
+// ramp moves the tile's spectrum off baseband, where the zero padding of a band-limited
+// interpolation would cut through it.  One block of kThreads threads; red holds 4 kWarps
+// doubles; ends with a barrier.
+__device__ inline void deramp_tile(float2* t, int stride, int n, double* red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float sr = 0.0f, si = 0.0f, lr = 0.0f, li = 0.0f;
+    for (int k = tid; k < n * n; k += kThreads) {
+        const int y = k / n, x = k - y * n;
+        const float2 z = t[y * stride + x];
+        if (x + 1 < n) {
+            const float2 w = t[y * stride + x + 1];
+            sr = fmaf(w.x, z.x, fmaf(w.y, z.y, sr));
+            si = fmaf(w.y, z.x, fmaf(-w.x, z.y, si));
+        }
+        if (y + 1 < n) {
+            const float2 w = t[(y + 1) * stride + x];
+            lr = fmaf(w.x, z.x, fmaf(w.y, z.y, lr));
+            li = fmaf(w.y, z.x, fmaf(-w.x, z.y, li));
+        }
+    }
+    double v[4] = {sr, si, lr, li};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) red[4 * warp + k] = v[k];
+    __syncthreads();
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < kWarps; ++w)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a[k] += red[4 * w + k];
+    const float ps = (float)atan2(a[1], a[0]), pl = (float)atan2(a[3], a[2]);
+    __syncthreads();
+    for (int k = tid; k < n * n; k += kThreads) {
+        const int y = k / n, x = k - y * n;
+        float s, c;
+        sincosf(fmaf(ps, (float)x, pl * (float)y), &s, &c);
+        const float2 z = t[y * stride + x];
+        t[y * stride + x] = make_float2(fmaf(z.x, c, z.y * s), fmaf(z.y, c, -z.x * s));
+    }
+    __syncthreads();
+}
+
 }  // namespace ampcor_b200

@@ -154,6 +154,29 @@ def plain_512():
     return Workload("plain_512", ref, tgt, ulhc, kept, 32, 8, 2, 4, 4, truth)
 
 
+def doppler_512(ramp=(0.1, 0.45), band=0.6, shift=(3.4, -2.7)):
+    """plain_512's geometry on oversampled speckle whose spectrum sits off baseband, as SAR data
+    with a Doppler centroid does: band-limited speckle (a fraction ``band`` of each axis'
+    spectrum), the secondary Fourier-shifted by ``shift`` px, both multiplied by the phase ramp
+    exp(2 pi i (ramp[0] line + ramp[1] sample)) (cycles per sample).  Without a deramp the
+    band-limited refinement's zero padding cuts through the shifted spectrum."""
+    base = speckle((512, 512), 0).astype(np.complex128)
+    B = np.fft.fft2(base)
+    fy = np.fft.fftfreq(512)[:, None]
+    fx = np.fft.fftfreq(512)[None, :]
+    B[(np.abs(fy) > band / 2) | (np.abs(fx) > band / 2)] = 0.0
+    base = np.fft.ifft2(B)
+    base /= np.sqrt((np.abs(base) ** 2).mean())
+    y, x = np.mgrid[0:512, 0:512]
+    ph = np.exp(2j * np.pi * (ramp[0] * y + ramp[1] * x))
+    ref = (ph * base).astype(np.complex64)
+    tgt = (ph * fourier_shift(base.astype(np.complex64), *shift)).astype(np.complex64)
+    centres = uniform_grid((512, 512), (8, 8))
+    ulhc, kept = _grid_pairs(ref.shape, centres, 32, 8)
+    truth = np.tile(np.array([list(shift)]), (len(kept), 1))
+    return Workload("doppler_512", ref, tgt, ulhc, kept, 32, 8, 2, 4, 4, truth)
+
+
 def _cached(key, make):
     os.makedirs(CACHE, exist_ok=True)
     path = os.path.join(CACHE, key + ".npy")

@@ -39,7 +39,7 @@ class Worker:
     """A correlator bound to one CUDA device."""
 
     def __init__(self, pairs, chip, window, refine_factor=2, refine_margin=8, zoom_factor=4,
-                 device=0, ref_compat=False, plain=False):
+                 device=0, ref_compat=False, plain=False, deramp=False):
         self._lib = _lib.load()
         chip = tuple(int(c) for c in chip)
         window = tuple(int(w) for w in window)
@@ -60,7 +60,8 @@ class Worker:
             refine_margin=self.refine_margin,
             zoom_factor=self.zoom_factor,
             device=self.device,
-            flags=(_lib.FLAG_REF_COMPAT if ref_compat else 0) | (_lib.FLAG_PLAIN_FP32 if plain else 0),
+            flags=(_lib.FLAG_REF_COMPAT if ref_compat else 0) | (_lib.FLAG_PLAIN_FP32 if plain else 0)
+            | (_lib.FLAG_DERAMP if deramp else 0),
         )
         handle = c_void_p()
         _check(self._lib, None, self._lib.ampcor_create(byref(params), byref(handle)))

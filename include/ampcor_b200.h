@@ -34,6 +34,11 @@ extern "C" {
 #define AMPCOR_FLAG_PLAIN_FP32 2u  /* correlate with FP32 fused multiply-adds (the plain form)
                                       instead of FFTs (the spectral form) or bf16x3 split
                                       products on the tensor cores */
+#define AMPCOR_FLAG_DERAMP 4u      /* remove each complex chip's and neighbourhood's linear phase
+                                      ramp (lag-one autocorrelation phases along samples and
+                                      lines) before the band-limited refinement; the reference's
+                                      _deramp (Sequential.icc:1094-1098) is an empty stub, placed
+                                      where a phase ramp could not change the amplitudes anyway */
 
 typedef struct ampcor_handle ampcor_handle;
 

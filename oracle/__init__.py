@@ -26,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_COMPAT = 1
+DERAMP = 2  # ORACLE_DERAMP: remove each complex tile's linear phase ramp before refining
 
 
 class Src(ctypes.Structure):
@@ -67,6 +68,8 @@ def load():
         lib.oracle_adjust.restype = None
         lib.oracle_adjust.argtypes = [POINTER(Src), c_longlong, POINTER(Geom), c_void_p,
                                       c_void_p, c_void_p, c_void_p, c_int]
+        lib.oracle_deramp.restype = None
+        lib.oracle_deramp.argtypes = [c_void_p, c_int]
         lib.oracle_argmax_first.restype = c_int
         lib.oracle_argmax_first.argtypes = [c_void_p, c_longlong]
         lib.oracle_sat.restype = None
@@ -123,11 +126,13 @@ def coarse_cpu(ref, tgt, ulhc, R, W, surfaces=False, threads=None):
     return (arg, gap, cor) if surfaces else (arg, gap)
 
 
-def adjust(ref, tgt, ulhc, R, W, f, m, z, ref_compat=False, surfaces=False, threads=None):
+def adjust(ref, tgt, ulhc, R, W, f, m, z, ref_compat=False, surfaces=False, threads=None,
+           deramp=False):
     """Full FP64 pipeline.  Returns (offsets (P,2) float32, diag structured (P,), [coarse and
-    refined surfaces])."""
+    refined surfaces]).  ``deramp`` removes each complex tile's linear phase ramp before the
+    refinement (oracle_deramp)."""
     s = Sources(ref, tgt, ulhc)
-    g = Geom(R, W, f, m, z, REF_COMPAT if ref_compat else 0)
+    g = Geom(R, W, f, m, z, (REF_COMPAT if ref_compat else 0) | (DERAMP if deramp else 0))
     C, Cf = W - R + 1, 2 * f * m + 1
     off = np.zeros((s.pairs, 2), np.float32)
     diag = np.zeros(s.pairs, DIAG_DTYPE)
@@ -140,6 +145,13 @@ def adjust(ref, tgt, ulhc, R, W, f, m, z, ref_compat=False, surfaces=False, thre
 
 
 # stage functions ------------------------------------------------------------------------
+
+def deramp(tile):
+    """The FP64 deramp of one square complex tile (oracle_deramp), returned as a new array."""
+    t = np.ascontiguousarray(tile, np.complex128).copy()
+    load().oracle_deramp(t.ctypes.data, t.shape[0])
+    return t
+
 
 def sat(x):
     x = np.ascontiguousarray(x, np.float64)

@@ -69,6 +69,7 @@ typedef struct {
 } oracle_geom;
 
 #define ORACLE_REF_COMPAT 1
+#define ORACLE_DERAMP 2     /* remove the linear phase ramp of each complex tile before refining */
 
 /* per-pair diagnostics */
 typedef struct {
@@ -357,6 +358,38 @@ void oracle_coarse_cpu(const oracle_src *src, i64 pairs, int R, int W,
 /* the full pipeline                                                                       */
 /* ------------------------------------------------------------------------------------- */
 
+/* The opt-in deramp before refinement, in FP64: phi_s = arg sum z(y, x+1) conj z(y, x),
+ * phi_l = arg sum z(y+1, x) conj z(y, x) over the N x N tile (interleaved complex), then
+ * z(y, x) *= exp(-i (phi_s x + phi_l y)).  The reference's _deramp (Sequential.icc:1094-1098) is an
+ * empty stub that runs after refinement, where a phase ramp cannot change the amplitudes. */
+void oracle_deramp(double *t, int N)
+{
+    double sr = 0.0, si = 0.0, lr = 0.0, li = 0.0;
+    for (int y = 0; y < N; ++y)
+        for (int x = 0; x < N; ++x) {
+            const double zr = t[2 * ((i64)y * N + x)], zi = t[2 * ((i64)y * N + x) + 1];
+            if (x + 1 < N) {
+                const double wr = t[2 * ((i64)y * N + x + 1)], wi = t[2 * ((i64)y * N + x + 1) + 1];
+                sr += wr * zr + wi * zi;
+                si += wi * zr - wr * zi;
+            }
+            if (y + 1 < N) {
+                const double wr = t[2 * ((i64)(y + 1) * N + x)], wi = t[2 * ((i64)(y + 1) * N + x) + 1];
+                lr += wr * zr + wi * zi;
+                li += wi * zr - wr * zi;
+            }
+        }
+    const double ps = atan2(si, sr), pl = atan2(li, lr);
+    for (int y = 0; y < N; ++y)
+        for (int x = 0; x < N; ++x) {
+            const double ph = ps * x + pl * y, c = cos(ph), sn = sin(ph);
+            double *z = t + 2 * ((i64)y * N + x);
+            const double zr = z[0], zi = z[1];
+            z[0] = zr * c + zi * sn;
+            z[1] = zi * c - zr * sn;
+        }
+}
+
 void oracle_adjust(const oracle_src *src, i64 pairs, const oracle_geom *g,
                    float *offsets, oracle_diag *diag, double *coarse_surfaces,
                    double *refined_surfaces, int threads)
@@ -367,6 +400,7 @@ void oracle_adjust(const oracle_src *src, i64 pairs, const oracle_geom *g,
     const int E = R + 2 * m;
     const int Rf = f * R, Wf = f * E, Cf = 2 * f * m + 1, Z = z * Cf;
     const int compat = (g->flags & ORACLE_REF_COMPAT) != 0;
+    const int deramp = (g->flags & ORACLE_DERAMP) != 0;
 
     double *Ur = (double *)malloc(sizeof(double) * (size_t)Rf * R);
     double *Ue = (double *)malloc(sizeof(double) * (size_t)Wf * E);
@@ -416,6 +450,7 @@ void oracle_adjust(const oracle_src *src, i64 pairs, const oracle_geom *g,
                     cin[2 * ((i64)i * R + j)] = px[0];
                     cin[2 * ((i64)i * R + j) + 1] = px[1];
                 }
+            if (deramp) oracle_deramp(cin, R);
             oracle_upsample(cin, R, f, Ur, cout, ctmp);
             for (i64 k = 0; k < (i64)Rf * Rf; ++k)
                 chip[k] = sqrt(cout[2 * k] * cout[2 * k] + cout[2 * k + 1] * cout[2 * k + 1]);
@@ -426,6 +461,7 @@ void oracle_adjust(const oracle_src *src, i64 pairs, const oracle_geom *g,
                     cin[2 * ((i64)i * E + j)] = px[0];
                     cin[2 * ((i64)i * E + j) + 1] = px[1];
                 }
+            if (deramp) oracle_deramp(cin, E);
             oracle_upsample(cin, E, f, Ue, cout, ctmp);
             for (i64 k = 0; k < (i64)Wf * Wf; ++k)
                 win[k] = sqrt(cout[2 * k] * cout[2 * k] + cout[2 * k + 1] * cout[2 * k + 1]);

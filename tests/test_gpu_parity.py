@@ -30,11 +30,11 @@ SURF_ATOL = 2e-5
 FORMS = ["spectral", "tensor", "plain"]
 
 
-def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor"):
+def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor", deramp=False):
     ulhc = w.ulhc if ulhc is None else ulhc
     worker = Worker(pairs=len(ulhc), chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
-                    zoom_factor=w.zoom_factor, plain=(form == "plain"))
+                    zoom_factor=w.zoom_factor, plain=(form == "plain"), deramp=deramp)
     if worker.form != form:
         worker.configure(form)
     assert worker.form == form
@@ -57,10 +57,10 @@ def run_device(w: synth.Workload, ulhc=None, surfaces=False, form="tensor"):
     return out
 
 
-def check_parity(w, ulhc, gpu, label):
+def check_parity(w, ulhc, gpu, label, deramp=False):
     R, W = w.chip, w.window
     off, od = oracle.adjust(w.ref, w.tgt, ulhc, R, W, w.refine_factor, w.refine_margin,
-                            w.zoom_factor)
+                            w.zoom_factor, deramp=deramp)
     arg, gap = oracle.coarse_cpu(w.ref, w.tgt, ulhc, R, W)
     d = gpu["diag"]
     # integer offsets against the reference CPU correlator
@@ -88,6 +88,16 @@ def check_parity(w, ulhc, gpu, label):
                                rtol=PEAK_RTOL, atol=0)
     np.testing.assert_allclose(d["coarse_peak"], od["coarse_peak"], rtol=PEAK_RTOL, atol=0)
     return off, od
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_deramp_parity(form):
+    # speckle off baseband (a Doppler ramp): with the opt-in deramp every form matches the FP64
+    # oracle's deramped pipeline and lands on the zoom grid's rounding of the applied shift
+    w = synth.doppler_512()
+    gpu = run_device(w, form=form, deramp=True)
+    check_parity(w, w.ulhc, gpu, f"doppler_512 deramp {form}", deramp=True)
+    assert np.abs(gpu["offsets"] - w.truth).max() <= 1.0 / 16 + 1e-6
 
 
 @pytest.mark.parametrize("form", FORMS)

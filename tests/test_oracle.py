@@ -154,3 +154,35 @@ def test_golden_plain_512():
     assert np.array_equal(off, g["offsets"])
     assert np.allclose(diag["refined_peak"], g["refined_peak"], rtol=1e-12, atol=0)
     assert np.array_equal(diag["fine_p"], g["fine_p"]) and np.array_equal(diag["fine_q"], g["fine_q"])
+
+
+def test_oracle_deramp_tile():
+    # a smooth field under a linear phase ramp: the deramp keeps every amplitude and leaves no
+    # phase step along lines or samples
+    n = 16
+    y, x = np.mgrid[0:n, 0:n]
+    rng = np.random.default_rng(0)
+    F = np.fft.fft2(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    F[4:-4, :] = 0
+    F[:, 4:-4] = 0
+    t = np.fft.ifft2(F) * np.exp(1j * (0.9 * x + 0.4 * y))
+    d = oracle.deramp(t)
+    np.testing.assert_allclose(np.abs(d), np.abs(t), atol=1e-12)
+    assert abs(np.angle((d[:, 1:] * np.conj(d[:, :-1])).sum())) < 1e-12
+    assert abs(np.angle((d[1:, :] * np.conj(d[:-1, :])).sum())) < 1e-12
+
+
+def test_oracle_deramp_restores_doppler_offsets():
+    # speckle off baseband: the zero-padded refinement alone misplaces the sub-pixel offsets, the
+    # deramp before it restores them to the zoom grid's rounding of the applied shift
+    from ampcor_b200 import synth
+
+    w = synth.doppler_512()
+    plain, _ = oracle.adjust(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4)
+    deramped, _ = oracle.adjust(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4, deramp=True)
+    quantum = 1.0 / 8
+    assert np.abs(plain - w.truth).mean() > 0.15
+    assert np.abs(deramped - w.truth).max() <= quantum / 2 + 1e-6
+    flat = synth.doppler_512(ramp=(0.0, 0.0))
+    a, _ = oracle.adjust(flat.ref, flat.tgt, flat.ulhc, 32, 48, 2, 4, 4)
+    assert np.array_equal(deramped, a)
