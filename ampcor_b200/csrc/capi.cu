@@ -1236,8 +1236,12 @@ int correlate_host_banded(ampcor_handle* h, const ampcor_job* j)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long granule = std::min<long long>(2LL * std::max(sms, 1), std::max<long long>(1, P / (4 * kHostBands)));
     long long up_r = 0, up_t = 0, boxes = 0, need_r = 0, need_t = 0, p0 = 0;
+    // the first group is one granule (its upload is the one nothing hides), the others share the
+    // rest evenly
+    const long long first = std::min(P, granule);
     for (int g = 0; g < kHostBands && p0 < P; ++g) {
-        long long p1 = (P * (g + 1) / kHostBands + granule / 2) / granule * granule;
+        long long p1 = g == 0 ? first
+                              : first + ((P - first) * g / (kHostBands - 1) + granule / 2) / granule * granule;
         if (g + 1 == kHostBands || p1 > P) p1 = P;
         if (p1 <= p0) continue;
         for (long long p = p0; p < p1; ++p) {

@@ -496,10 +496,10 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 // rows whose first step reads the N-point spectra padded on the fly (N x F, rows upsampled);
 // N-point FFTs down the columns; then CB columns at a time the F-point inverses, again padding on
 // the fly, and the amplitudes out.  Scaled by 1 / N^2.
-template <int N1, int N2, int F1, int F2, int CB>
+template <int N1, int N2, int F1, int F2, int CB, bool DERAMP>
 __device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
                              const float2* __restrict__ twn_g, const float2* __restrict__ twf_g,
-                             float* __restrict__ out, int deramp)
+                             float* __restrict__ out)
 {
     constexpr int N = N1 * N2, F = F1 * F2;
     constexpr int RSN = N + 1, RSF = F + 1, CBS = CB + 1;
@@ -516,7 +516,7 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     cp_async_wait_all();
     __syncthreads();
     // the upsampled-rows buffer is free until the rows are written: the deramp's scratch
-    if (deramp) deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
+    if (DERAMP) deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
     // rows: forward N
     for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % N) * RSN, 1, t / N, twn);
     __syncthreads();
@@ -571,12 +571,12 @@ struct UpsampleGeom {
 
 // one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window; two CTAs
 // per SM where their shared memory allows
-template <int N1, int N2, int F1, int F2>
+template <int N1, int N2, int F1, int F2, bool DERAMP>
 __global__ void __launch_bounds__(kThreads, UpsampleGeom<N1, N2, F1, F2>::smem <= 113 * 1024 ? 2 : 1)
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
-                   long long out_off, int deramp)
+                   long long out_off)
 {
     extern __shared__ __align__(16) unsigned char rsm[];
     if (blockIdx.x >= pairs) return;
@@ -587,8 +587,8 @@ spec_refine_kernel(const float2* base, const long long* off, long long stride,
         const CoarseOut co = coarse[p];
         src += co.top * stride + co.left;
     }
-    fft_upsample<N1, N2, F1, F2, UpsampleGeom<N1, N2, F1, F2>::CB>(
-        src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off, deramp);
+    fft_upsample<N1, N2, F1, F2, UpsampleGeom<N1, N2, F1, F2>::CB, DERAMP>(
+        src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off);
 }
 
 // refinement (N, F = 2 N) pairs that are compiled: N, N1, N2, F1, F2
@@ -794,12 +794,15 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
                                const float2* twn, const float2* twf, float* refined,
                                long long refined_stride, long long out_off, int deramp)
 {
-#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                     \
-    if (n == NN) {                                                                             \
-        spec_refine_kernel<A, B, C, D><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
-            base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride,  \
-            out_off, deramp);                                                                  \
-        return cudaGetLastError();                                                             \
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                           \
+    if (n == NN) {                                                                                   \
+        if (deramp)                                                                                  \
+            spec_refine_kernel<A, B, C, D, true><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
+        else                                                                                         \
+            spec_refine_kernel<A, B, C, D, false><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
+        return cudaGetLastError();                                                                   \
     }
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
 #undef AMPCOR_REFINE_CASE
@@ -812,7 +815,9 @@ cudaError_t spec_set_smem_limits()
     cudaError_t e = cudaFuncSetAttribute(box_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D) \
     if (e == cudaSuccess)                  \
-        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess)                  \
+        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
 #undef AMPCOR_REFINE_CASE
 #define AMPCOR_SPEC_CASE(NN, A, B) \
