@@ -14,7 +14,7 @@
 //
 // Operands sit in shared memory as K-major core matrices (8 rows x 16 bytes, no swizzle): row r,
 // element k of a plane at float offset ((r / 8) KC + k / 4) 32 + (r % 8) 4 + k % 4, KC = 16-byte
-// chunks per row.  One CTA of 256 threads per SM walks the pairs of a chunk; lane 0 of warp 0
+// chunks per row.  One CTA of 256 threads per SM walks the pairs of a chunk; lane 0 of warp 7
 // issues the MMAs, all eight warps read accumulators (warps w and w + 4 share lane quarter w).
 // Every wait on an mbarrier is bounded; on expiry the kernel records an error, drains its MMAs
 // and frees its tensor memory.
@@ -28,6 +28,9 @@ namespace {
 
 constexpr int kZThreads = 256;
 constexpr int kZBatch = 3;  // 16-column accumulator loads in flight per thread
+// the thread that issues every MMA (and the drain after an expired wait): lane 0 of the last
+// warp, whose warp group reads fewer accumulator chunks per unit than the first one
+constexpr int kIssuer = kZThreads - 32;
 
 // accumulator row of this thread in a tile of M rows: M = 128 puts row r in lane r, M = 64 puts
 // rows 16q .. 16q+15 in lanes 32q .. 32q+15; -1 for lanes that hold no row
@@ -142,7 +145,7 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         __syncthreads();
 
         // T^T = U G^T: every row tile at once, tile mt at accumulator column 64 mt
-        if (tid == 0) {
+        if (tid == kIssuer) {
             tc_fence_after();
             for (int mt = 0; mt < zt.mtiles; ++mt) {
                 const int M = (mt == zt.mtiles - 1) ? zt.last_m : 128;
@@ -204,10 +207,10 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         };
         float bv = -INFINITY;
         int bi = INT_MAX;
-        if (tid == 0 && units > 0 && !*err) issue_unit(0);
+        if (tid == kIssuer && units > 0 && !*err) issue_unit(0);
         for (int un = 0; un < units; ++un) {
             if (*err) break;
-            if (tid == 0 && un + 1 < units) issue_unit(un + 1);
+            if (tid == kIssuer && un + 1 < units) issue_unit(un + 1);
             __syncwarp();
             const bool odd = (un & 1) != 0;
             const bool ok = mbar_wait(ubar + (un & 1), odd ? uph1 : uph0, err);
@@ -285,7 +288,7 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
 
     // teardown: after an expired wait, let the issued MMAs finish before freeing their memory
     __syncthreads();
-    if (*err && issued && tid == 0) {
+    if (*err && issued && tid == kIssuer) {
         mma_commit(drain);
         volatile int spare = 0;
         mbar_wait(drain, 0u, &spare);
