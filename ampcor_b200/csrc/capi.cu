@@ -552,7 +552,9 @@ int ensure_refined(ampcor_handle* h)
         return fail(h, AMPCOR_E_NOMEM, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
     }
     const size_t n = h->chunk;
-    if (h->form != kFormPlain &&
+    // per-pair placement statistics: only the tensor-core form stages them in memory (the
+    // spectral form takes them from the raster or computes them in the correlation kernel)
+    if (h->form == kFormTensor &&
         (cudaMalloc(&h->d_inv_c, n * h->C * h->C * sizeof(float)) != cudaSuccess ||
          cudaMalloc(&h->d_inv_f, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess))
         return fail(h, AMPCOR_E_NOMEM, "allocating placement statistics scratch");
