@@ -673,9 +673,10 @@ box_vsum_kernel(const float* __restrict__ a, long long samples, int R, long long
     }
 }
 
-// one CTA per box row: FP64 exclusive prefix sums of the row's column sums (in chunks of eight per
-// thread, a fixed order), then the box of every x from two prefix differences
-__global__ void __launch_bounds__(kThreads)
+// one CTA per box row: FP64 exclusive prefix sums of the row's column sums (in chunks of four per
+// thread, a fixed order), then the box of every x from two prefix differences; two CTAs per SM,
+// so that one row's loads overlap another's scan
+__global__ void __launch_bounds__(kThreads, 2)
 box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, long long row_lo,
                long long row_hi, long long samples, int R, float* __restrict__ inv)
 {
@@ -689,11 +690,12 @@ box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, lon
     const double* r1 = v1 + y * samples;
     const double* r2 = v2 + y * samples;
     double carry1 = 0.0, carry2 = 0.0;
-    for (long long c0 = 0; c0 < samples; c0 += kThreads * 8) {
-        const long long b0 = c0 + (long long)tid * 8;
-        double l1[8], l2[8], s1 = 0.0, s2 = 0.0;
+    constexpr int kPer = 4;  // consecutive samples per thread and chunk
+    for (long long c0 = 0; c0 < samples; c0 += kThreads * kPer) {
+        const long long b0 = c0 + (long long)tid * kPer;
+        double l1[kPer], l2[kPer], s1 = 0.0, s2 = 0.0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < kPer; ++k) {
             const long long i = b0 + k;
             const double p = i < samples ? __ldg(r1 + i) : 0.0;
             const double q = i < samples ? __ldg(r2 + i) : 0.0;
@@ -728,7 +730,7 @@ box_inv_kernel(const double* __restrict__ v1, const double* __restrict__ v2, lon
         }
         const double o1 = carry1 + w1 + (i1 - s1), o2 = carry2 + w2 + (i2 - s2);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < kPer; ++k) {
             const long long i = b0 + k;
             if (i < samples) {
                 P1[i] = o1 + l1[k];
