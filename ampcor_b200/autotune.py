@@ -1,9 +1,10 @@
 """Autotuner of the correlator.
 
 For one worker geometry (chip, window, refinement and zoom) it times every candidate
-configuration - correlation form (bf16x3 tensor-core or plain FP32) x refinement chunk (pairs
-refined per pass, which sets how much of the refine -> fine hand-off stays in L2) - on the
-caller's own device-resident batch and keeps the fastest.  Results are cached per device name and
+configuration - correlation form (spectral, bf16x3 tensor-core or plain FP32) x refinement chunk
+(pairs per pass of the pipeline: larger chunks mean fewer launches and whole waves, smaller ones
+keep more of the refine -> fine hand-off in L2) - on the caller's own device-resident batch and
+keeps the fastest.  Results are cached per device name and
 geometry in a JSON file (``AMPCOR_TUNE_CACHE``, default ``~/.cache/ampcor_b200/tune.json``).
 """
 from __future__ import annotations
@@ -11,7 +12,7 @@ from __future__ import annotations
 import json
 import os
 
-DEFAULT_CHUNKS = (296, 592, 1184, 2368)
+DEFAULT_CHUNKS = (296, 592, 1184, 2368, 4736, 9472, 18944)
 
 
 def _cache_path():
@@ -61,8 +62,14 @@ def tune(worker, ref, tgt, ulhc, forms=("spectral", "tensor", "plain"), chunks=D
         return dict(choice, cached=True)
     out = torch.empty((ulhc.shape[0], 2), dtype=torch.float32, device=ref.device)
     results = []
+    pairs = int(ulhc.shape[0])
     for form in forms:
-        for chunk in chunks:
+        whole = False  # a chunk of at least the whole batch has been timed for this form
+        for chunk in sorted(chunks):
+            if chunk >= pairs:
+                if whole:
+                    continue
+                whole = True
             try:
                 worker.configure(form, chunk)
             except Error:
