@@ -1198,10 +1198,10 @@ int ampcor_synchronize(ampcor_handle* h, void* stream)
     return AMPCOR_OK;
 }
 
-// A host-buffer job of the spectral form in at most kHostBands groups of consecutive pairs, growing
-// from one wave: group g needs
-// the raster rows up to the deepest chip and window of pairs 0 .. end of g (so pairs in raster
-// order need about a band each); those rows go up on the copy stream while the compute stream
+// A host-buffer job of the spectral form in at most kHostBands groups of consecutive pairs,
+// growing from one wave: group g needs the raster rows up to the deepest chip and window of
+// pairs 0 .. end of g (so pairs in raster order need about a band each); those rows go up on
+// the copy stream while the compute stream
 // correlates group g - 1, then the compute stream detects the new rows, extends the box
 // statistics to the box rows they complete and correlates group g.  Same kernels and the same
 // values as one upload followed by the whole job; the upload hides behind all but the first band.
