@@ -1240,14 +1240,13 @@ int correlate_host_banded(ampcor_handle* h, const ampcor_job* j)
     const long long granule = std::min<long long>(2LL * std::max(sms, 1), std::max<long long>(1, P / (4 * kHostBands)));
     long long up_r = 0, up_t = 0, boxes = 0, need_r = 0, need_t = 0, p0 = 0;
     // the first group is one granule (its upload is the one nothing hides); each next group is
-    // half as large again as the one before (its rows go up while the one before is correlated,
-    // and uploading a pair's rows takes about half as long as correlating it), the last takes
-    // the rest
+    // twice the one before (its rows go up while the one before is correlated, and uploading a
+    // pair's rows takes about half as long as correlating it), the last takes the rest
     long long size = std::min(P, granule);
     for (int g = 0; g < kHostBands && p0 < P; ++g) {
         long long p1 = p0 + (size + granule / 2) / granule * granule;
         if (g + 1 == kHostBands || p1 > P) p1 = P;
-        size = size * 3 / 2;
+        size = size * 2;
         if (p1 <= p0) continue;
         for (long long p = p0; p < p1; ++p) {
             need_r = std::max<long long>(need_r, std::min<long long>((long long)j->ulhc[4 * p] + h->R, rlines));
