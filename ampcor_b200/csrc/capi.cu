@@ -1467,8 +1467,10 @@ const char* ampcor_copyright(void) { return kCopyright; }
 // cudaMalloc fails or fragments it), and real-time or on-board processing chains that forbid any
 // allocation after start-up.  ampcor_correlate_noalloc() serves them: every intermediate of the
 // pipeline lives in the fixed device array below, which the CUDA runtime creates when it loads
-// this library on a device and keeps until the process exits (kNoAllocBytes on every device that
-// loads the library).  The array is shared by all calls; calls that overlap on the GPU race.
+// this library's device code on a device (with lazy module loading, at the first call that needs
+// it: a call with no pairs at start-up does that and launches nothing) and keeps until the process
+// exits (kNoAllocBytes per device).  The array is shared by all calls; calls that overlap on the
+// GPU race.  Every call waits for its stream, so none runs on a capturing stream.
 // ------------------------------------------------------------------------------------------
 
 namespace {
@@ -1535,7 +1537,7 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
                             "ampcor_correlate_noalloc takes at most 16384 pairs per call");
     if (j->pairs && (!j->ref || !j->tgt || !j->ulhc || !j->offsets))
         return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "null raster, corner or offset pointer");
-    if (j->ref_lines <= 0 || j->ref_samples <= 0 || j->tgt_lines <= 0 || j->tgt_samples <= 0)
+    if (j->pairs && (j->ref_lines <= 0 || j->ref_samples <= 0 || j->tgt_lines <= 0 || j->tgt_samples <= 0))
         return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "empty raster");
     if (p->device < 0 || p->device >= kNoAllocMaxDevices)
         return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG, "device ordinal out of range");
@@ -1576,8 +1578,21 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "cudaSetDevice", e);
     cudaStream_t st = (cudaStream_t)stream;
+    // every call waits for its stream before it returns, which a capturing stream does not allow
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &capture)) != cudaSuccess)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "querying the stream", e);
+    if (capture != cudaStreamCaptureStatusNone)
+        return noalloc_fail(errbuf, errlen, AMPCOR_E_ARG,
+                            "ampcor_correlate_noalloc waits for its stream and cannot run on a capturing stream");
 
     std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    // a failure once work is queued still waits for the stream, so that the shared array is idle
+    // whenever the lock is released
+    auto queued_fail = [&](int code, const char* what, cudaError_t qe) {
+        cudaStreamSynchronize(st);
+        return noalloc_fail(errbuf, errlen, code, what, qe);
+    };
     // the device address of the fixed array, looked up once per device with that device current
     if (!g_noalloc_base[p->device]) {
         void* base = nullptr;
@@ -1599,6 +1614,8 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
         (e = cudaFuncSetAttribute(fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem)) != cudaSuccess)
         return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "configuring kernel shared memory", e);
+    // an empty batch only loads the device code and looks up the array (a start-up call)
+    if (j->pairs == 0) return AMPCOR_OK;
 
     // tap tables: computed on the host into a fixed buffer; a copy from pageable memory has left
     // the buffer when cudaMemcpyAsync returns, so the buffer is free again under the lock
@@ -1607,11 +1624,10 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
     taps_fill(Cf, z, 0, zg.taps_len, g_noalloc_taps + chip_taps + win_taps);
     if ((e = cudaMemcpyAsync(taps, g_noalloc_taps, (chip_taps + win_taps + zoom_taps) * sizeof(float),
                              cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "uploading interpolation taps", e);
+        return queued_fail(AMPCOR_E_CUDA, "uploading interpolation taps", e);
     // the bounds counter keeps the previous call's value: clear it
     if ((e = cudaMemsetAsync(bad, 0, sizeof(unsigned int), st)) != cudaSuccess)
-        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "clearing the bounds counter", e);
-    if (j->pairs == 0) return AMPCOR_OK;
+        return queued_fail(AMPCOR_E_CUDA, "clearing the bounds counter", e);
 
     const long long P = (long long)j->pairs;
     pair_offsets_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
@@ -1633,11 +1649,11 @@ extern "C" int ampcor_correlate_noalloc(const ampcor_params* p, const ampcor_job
             reinterpret_cast<PairDiag*>(j->diag), j->refined_surfaces);
     }
     if ((e = cudaGetLastError()) != cudaSuccess)
-        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "launching the correlation kernels", e);
+        return queued_fail(AMPCOR_E_CUDA, "launching the correlation kernels", e);
     unsigned int nbad = 0;
     if ((e = cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
-        return noalloc_fail(errbuf, errlen, AMPCOR_E_CUDA, "running the correlation pipeline", e);
+        return queued_fail(AMPCOR_E_CUDA, "running the correlation pipeline", e);
     if (nbad)
         return noalloc_fail(errbuf, errlen, AMPCOR_E_BOUNDS,
                             "tile pair(s) leave their raster; their offsets are NaN");

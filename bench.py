@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -32,6 +33,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# nvidia-smi clock samples of the timed region (AMPCOR_CLOCK_DIR, else the system temp dir)
+CLOCK_DIR = os.environ.get("AMPCOR_CLOCK_DIR") or tempfile.gettempdir()
 METRIC = "tile pairs/s (64² chip, ±32 px search) & p99 job latency at ≤0.01 px error"
 UNIT = "tile pairs/s"
 
@@ -111,7 +114,7 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(CLOCK_DIR, f"ampcor_clocks_rank{index}.csv")
 
     def start(self):
         try:
@@ -478,11 +481,6 @@ def uneven_run(device, args):
     }
     ub.close()
     return out
-
-
-def worker_chunk():
-    env = os.environ.get("AMPCOR_CHUNK")
-    return int(env) if env and int(env) > 0 else 148 * 4
 
 
 def main():

@@ -168,12 +168,18 @@ int ampcor_stage_times(ampcor_handle* handle, double* coarse_ms, double* refine_
    allocation after start-up.  No reference counterpart.
    params gives the geometry and the device (params->pairs is ignored); every pointer of job is
    device memory on that device; the work runs on stream (a cudaStream_t, NULL for the legacy
-   default stream) and the call waits for it.  All intermediates live in one fixed device array of
-   about 41 MiB that every device loading this library holds until the process exits; a call
-   takes at most 16384 pairs (more returns AMPCOR_E_ARG).  The first call on a device looks up the
-   array's device address, so make that first call before any stream capture.  All calls share
-   the array: calls that overlap on the GPU (other threads, other streams) race and must be
-   serialised by the caller.  A failure message, if errbuf is not NULL, is written to errbuf
+   default stream) and every call waits for that stream to finish before it returns (it reads the
+   bounds counter back to the host), so a stream that is being captured into a CUDA graph is
+   refused with AMPCOR_E_ARG.  All intermediates live in one fixed device array of about 41 MiB;
+   a call takes at most 16384 pairs (more returns AMPCOR_E_ARG).  The CUDA runtime creates the
+   array when this library's device code is first loaded on a device (with lazy module loading,
+   at the first call that needs it), so make one call with job->pairs == 0 at start-up, before
+   the application's own pool takes the GPU: it loads the device code, looks up the array's
+   address and launches nothing; from then on the device holds the array until the process
+   exits.  All calls share the array: calls that overlap on the GPU (other processes, or
+   streams the caller does not order) race and must be serialised by the caller; calls from
+   threads of one process are serialised by a lock, and a failed call still waits for its stream
+   before it releases the lock.  A failure message, if errbuf is not NULL, is written to errbuf
    (errlen bytes). */
 int ampcor_correlate_noalloc(const ampcor_params* params, const ampcor_job* job, void* stream,
                              char* errbuf, size_t errlen);

@@ -26,6 +26,30 @@ def test_plan_corners_and_validity():
     assert ulhc.tolist() == [[16, 16, 34 - 16 - 8, 29 - 16 - 8]]
 
 
+def test_offset_map_product():
+    # pkg/ampcor/dom/OffsetMap.py:14-95 (grid-indexed domain/codomain, row-major by default) and
+    # Grid.py:34-50 (coarse map from a uniform grid and a constant shift); the refined map moves
+    # each valid pair's target point by its offset, dropped pairs stay without a target
+    coarse = plan.coarse_map((3, 4), (128, 160), shift=(2, -3))
+    assert len(coarse) == 12 and coarse.offset((1, 2)) == 6 and coarse.index(6) == (1, 2)
+    assert coarse[(0, 0)] == ((22, 20), (24, 17))
+    colmajor = plan.OffsetMap((3, 4), layout=(0, 1))
+    assert colmajor.offset((1, 2)) == 7 and colmajor.index(7) == (1, 2)
+    ulhc, valid = plan.plan_pairs(coarse.domain, coarse.codomain, (32, 32), (8, 8), (128, 160),
+                                  (128, 160))
+    offs = np.stack([np.arange(valid.sum()) * 0.25, -np.arange(valid.sum()) * 0.5], 1)
+    offs[1] = np.nan  # a pair whose tiles left a raster
+    fine = plan.refined_map(coarse, valid, offs)
+    field = fine.field()
+    assert field.shape == (3, 4, 2)
+    k = np.flatnonzero(valid)
+    want = np.full((12, 2), np.nan)
+    want[k] = np.array([2.0, -3.0]) + offs
+    np.testing.assert_array_equal(field.reshape(12, 2), want.astype(np.float32))
+    with pytest.raises(IndexError):
+        coarse[(3, 0)]
+
+
 def test_production_grid_is_full():
     w = synth.production_4096()
     assert w.pairs == 14400

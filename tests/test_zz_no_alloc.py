@@ -77,6 +77,35 @@ def test_noalloc_matches_regular_entry_point_twice_in_a_row():
         np.testing.assert_array_equal(diag, want[1])
 
 
+def test_noalloc_start_up_call_and_bounds():
+    # a call with no pairs is the start-up call (loads the device code, launches nothing); a pair
+    # whose window leaves its raster gives AMPCOR_E_BOUNDS and NaN offsets for that pair only,
+    # and the next clean call returns OK because each call clears the shared bounds counter
+    lib = _lib.load()
+    w = synth.plain_512()
+    err = ctypes.create_string_buffer(256)
+    empty = _lib.Job(ref=None, ref_lines=0, ref_samples=0, tgt=None, tgt_lines=0, tgt_samples=0,
+                     ulhc=None, pairs=0, offsets=None)
+    assert lib.ampcor_correlate_noalloc(ctypes.byref(params_of(w)), ctypes.byref(empty), None, err,
+                                        len(err)) == _lib.OK, err.value.decode()
+    ulhc = w.ulhc[:4].copy()
+    ulhc[2, 2] = 500   # window leaves the 512-line raster
+    ref, tgt, u = device_batch(w, ulhc)
+    off = torch.zeros((4, 2), dtype=torch.float32, device=ref.device)
+    job = _lib.Job(ref=ref.data_ptr(), ref_lines=512, ref_samples=512, tgt=tgt.data_ptr(),
+                   tgt_lines=512, tgt_samples=512, ulhc=u.data_ptr(), pairs=4,
+                   offsets=off.data_ptr())
+    st = ctypes.c_void_p(torch_stream_handle(None, ref.device))
+    rc = lib.ampcor_correlate_noalloc(ctypes.byref(params_of(w)), ctypes.byref(job), st, err,
+                                      len(err))
+    assert rc == _lib.E_BOUNDS and b"leave their raster" in err.value
+    o = off.cpu().numpy()
+    assert np.isnan(o[2]).all() and np.isfinite(o[[0, 1, 3]]).all()
+    got, _ = run_noalloc(w, w.ulhc[:4])
+    want, _ = run_regular(w, w.ulhc[:4])
+    np.testing.assert_array_equal(got, want)
+
+
 def test_noalloc_rejects_too_many_pairs():
     lib = _lib.load()
     w = synth.plain_512()
