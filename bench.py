@@ -378,13 +378,9 @@ def run_b200(args):
         top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
         topk = kernels[top]
         cpu = None
+        parity_rep = None
         if world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            rate, n, dt = oracle_rate(w, args.cpu_seconds, threads)
-            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": (f"FP64 restatement of the full reference pipeline (oracle/oracle.c) "
-                              f"on {n} random pairs of the workload, {dt:.1f} s on {threads} "
-                              f"threads")}
+            cpu, parity_rep = cpu_leg(w, worker, ref, tgt, ulhc, offsets)
         h2d = w.ref.nbytes + w.tgt.nbytes + w.ulhc.nbytes
         d2h = w.pairs * 2 * 4
         line = {
@@ -419,6 +415,8 @@ def run_b200(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if parity_rep:
+            line["parity"] = parity_rep
         if world == 1 and not args.no_serving:
             line["serving"] = serving_run(local, args)
         if world == 1 and not args.no_uneven:
@@ -428,6 +426,45 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def cpu_leg(w, worker, ref, tgt, ulhc, timed_offsets):
+    """The CPU baseline and the parity check of the timed job, outside the timed region: the
+    FP64 oracle runs the whole job once on all host threads (its time is the baseline), and the
+    timed job's offsets are checked against it pair by pair (oracle.parity.compare; the same
+    worker reruns the job with diagnostics and surfaces, and its offsets must equal the timed
+    ones bit for bit)."""
+    import torch
+
+    from oracle import parity
+    from ampcor_b200.worker import DIAG_DTYPE
+
+    dev = ref.device
+    P = w.pairs
+    diag = torch.zeros((P, DIAG_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    cs = torch.zeros((P, worker.coarse_dim, worker.coarse_dim), dtype=torch.float32, device=dev)
+    rs = torch.zeros((P, worker.refined_dim, worker.refined_dim), dtype=torch.float32, device=dev)
+    off = worker.correlate(ref, tgt, ulhc, diag=diag, coarse_surfaces=cs, refined_surfaces=rs)
+    same_as_timed = bool(torch.equal(off, timed_offsets))
+    gpu_off = timed_offsets.cpu().numpy()
+    gpu_diag = diag.cpu().numpy().view(DIAG_DTYPE).reshape(P)
+    cs_h, rs_h = cs.cpu().numpy(), rs.cpu().numpy()
+    del cs, rs
+    threads = os.cpu_count() or 1
+    orc = parity.oracle_run(w.ref, w.tgt, w.ulhc, w.chip, w.window, w.refine_factor,
+                            w.refine_margin, w.zoom_factor, threads=threads)
+    dt = orc["adjust_seconds"]
+    cpu = {"value": P / dt, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": (f"the whole job ({P} pairs) through the FP64 restatement of the full "
+                      f"reference pipeline (oracle/oracle.c: coarse NCC, nudge, FFT refinement, "
+                      f"refined NCC, zoom, offsets), OpenMP over pairs, {dt:.1f} s on {threads} "
+                      f"threads")}
+    rep = parity.summary(parity.compare(orc, gpu_off, gpu_diag, cs_h, rs_h))
+    rep["rerun_equals_timed_offsets"] = same_as_timed
+    rep["rule"] = ("every pair against the FP64 oracle: cells equal (offsets then bit-exact) "
+                   "unless the pair's own measured surface error explains a near-tie, counted "
+                   "in pairs_excused; oracle/parity.py")
+    return cpu, rep
 
 
 def serving_run(device, args):

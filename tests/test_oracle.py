@@ -9,6 +9,7 @@ import pytest
 import oracle
 from oracle import npref
 from ampcor_b200 import synth
+from ampcor_b200.worker import DIAG_DTYPE
 
 from fixtures import placement_identity
 
@@ -186,3 +187,40 @@ def test_oracle_deramp_restores_doppler_offsets():
     flat = synth.doppler_512(ramp=(0.0, 0.0))
     a, _ = oracle.adjust(flat.ref, flat.tgt, flat.ulhc, 32, 48, 2, 4, 4)
     assert np.array_equal(deramped, a)
+
+
+def test_parity_checker_rules():
+    # the pair-by-pair checker on CPU: the oracle's own results (as float32) pass with nothing
+    # excused; a coarse cell moved on a pair with a clear maximum fails; moving the cell of the
+    # pair with the smallest top-two gap is excused when its surface error explains the gap
+    from oracle import parity
+
+    w = synth.plain_512()
+    orc = parity.oracle_run(w.ref, w.tgt, w.ulhc, 32, 48, 2, 4, 4)
+    od = orc["diag"]
+    gd = np.zeros(len(od), dtype=DIAG_DTYPE)
+    for k in ("coarse_u", "coarse_v", "top", "left", "fine_p", "fine_q"):
+        gd[k] = od[k]
+    gd["refined_peak"] = od["refined_peak"]
+    gd["coarse_peak"] = od["coarse_peak"]
+    cs = orc["coarse"].astype(np.float32)
+    rs = orc["refined"].astype(np.float32)
+    rep = parity.compare(orc, orc["offsets"], gd, cs, rs)
+    assert rep["failures"] == [] and rep["pairs_excused"] == 0 and rep["pairs_checked"] == 64
+    assert rep["max_abs_err_vs_oracle_px"] == 0.0
+    bad = gd.copy()
+    bad["coarse_v"][5] += 1
+    rep = parity.compare(orc, orc["offsets"], bad, cs, rs)
+    assert [f[0] for f in rep["failures"]][:1] == [5]
+    # a near-tie: make pair p's second-best coarse cell win, with a surface error that covers it
+    p = int(np.argmin(od["coarse_gap"]))
+    C = 17
+    surf = orc["coarse"][p].reshape(-1)
+    k2 = int(np.argsort(surf)[-2])
+    tie = gd.copy()
+    tie["coarse_u"][p], tie["coarse_v"][p] = divmod(k2, C)
+    cs2 = cs.copy()
+    cs2[p].reshape(-1)[k2] += np.float32(od["coarse_gap"][p])
+    rep = parity.compare(orc, orc["offsets"], tie, cs2, rs)
+    coarse_fail = [f for f in rep["failures"] if "coarse cell" in f[1]]
+    assert coarse_fail == [] and rep["coarse_cells_differing"] == 1
