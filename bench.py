@@ -13,9 +13,12 @@ pairs of all ranks divided by the slowest rank's device time.
 (ampcor_correlate_host): each step uploads both rasters and the corners from pinned host
 memory, runs the job and reads the offsets back.
 
-``--impl reference`` times the CPU implementation of the path instead: the FP64 restatement of
-the reference pipeline in oracle/ (the reference itself cannot be built here: it needs the pyre
-framework), with all host threads, on a bounded sample of the same pairs each step.
+``--impl reference`` times the reference's own CPU implementation of the path instead: its
+``Sequential`` correlator (lib/libampcor/correlators/Sequential.cc, the coarse correlation; its
+refine() is empty), compiled unmodified into oracle/_ref/ against stand-ins of pyre, driven
+through its own addReferenceTile / addTargetTile / adjust on tiles of the same rasters, one worker
+per host thread, on a bounded sample of the same pairs each step.  Where oracle/_ref is not built
+it times the FP64 restatement of the full pipeline in oracle/ instead (``kind: port``).
 """
 from __future__ import annotations
 
@@ -104,6 +107,32 @@ def oracle_rate(w, seconds, threads):
     return n / dt, n, dt
 
 
+def reference_rate(w, rasters, seconds, threads):
+    """Pairs/s of the reference's own CPU correlator (oracle/_ref) on a bounded sample of the
+    workload's pairs; ``rasters`` holds the raster files it reads (written before timing)."""
+    from oracle import ref as refcpu
+
+    rng = np.random.default_rng(0)
+    order = rng.permutation(w.pairs)
+    probe = np.sort(order[: max(threads, 8)])
+    t0 = time.perf_counter()
+    refcpu.sequential(rasters, w.ulhc[probe], w.chip, w.window, threads=threads)
+    per = (time.perf_counter() - t0) / len(probe)
+    n = int(min(w.pairs, max(len(probe), seconds / max(per, 1e-9))))
+    n = max(threads, (n // threads) * threads) if n >= threads else n
+    sample = np.sort(order[:n])
+    t0 = time.perf_counter()
+    refcpu.sequential(rasters, w.ulhc[sample], w.chip, w.window, threads=threads)
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+REFERENCE_SAMPLE = ("the reference's own CPU correlator (lib/libampcor/correlators/Sequential.cc "
+                    "adjust(), FP64 coarse correlation, with its addReferenceTile/addTargetTile "
+                    "reading the rasters as SLC files), compiled unmodified into oracle/_ref/ "
+                    "against stand-ins of pyre, one worker per thread")
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples while the timed region runs."""
 
@@ -179,6 +208,7 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    from oracle import ref as refcpu
     from ampcor_b200 import synth
 
     w = synth.workload(args.workload)
@@ -186,23 +216,31 @@ def run_reference(args):
     total_budget = 150.0
     per_step = max(2.0, total_budget / max(1, args.steps + args.warmup))
     rates, samples = [], []
+    use_ref = refcpu.available()
+    rasters = refcpu.Rasters(w.ref, w.tgt) if use_ref else None
     for i in range(args.warmup + args.steps):
-        r, n, dt = oracle_rate(w, per_step, threads)
+        if use_ref:
+            r, n, dt = reference_rate(w, rasters, per_step, threads)
+        else:
+            r, n, dt = oracle_rate(w, per_step, threads)
         if i >= args.warmup:
             rates.append(r)
             samples.append(n)
+    if rasters:
+        rasters.close()
     value = statistics.median(rates)
+    what = (REFERENCE_SAMPLE if use_ref else
+            "FP64 restatement of the full reference pipeline (oracle/oracle.c: coarse NCC, nudge, "
+            "FFT refinement, refined NCC, zoom, offsets), OpenMP over pairs")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * w.pairs / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(w),
         "cpu_baseline": {
-            "value": value, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"FP64 restatement of the full reference pipeline (oracle/oracle.c: coarse "
-                       f"NCC, nudge, FFT refinement, refined NCC, zoom, offsets), OpenMP over pairs "
-                       f"on {threads} threads, {samples[0]} random pairs of the workload per step "
-                       f"(median of {len(rates)} steps)"),
+            "value": value, "unit": UNIT, "cores": threads, "kind": "reference" if use_ref else "port",
+            "sample": (f"{what}, on {threads} threads, {samples[0]} random pairs of the workload per "
+                       f"step (median of {len(rates)} steps); ms_per_step is the whole job at that rate"),
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -429,15 +467,18 @@ def run_b200(args):
 
 
 def cpu_leg(w, worker, ref, tgt, ulhc, timed_offsets):
-    """The CPU baseline and the parity check of the timed job, outside the timed region: the
-    FP64 oracle runs the whole job once on all host threads (its time is the baseline), and the
-    timed job's offsets are checked against it pair by pair (oracle.parity.compare; the same
-    worker reruns the job with diagnostics and surfaces, and its offsets must equal the timed
-    ones bit for bit)."""
+    """The CPU baseline and the parity check of the timed job, outside the timed region.  The
+    baseline is the reference's own CPU correlator (oracle/_ref) on a bounded sample of the job's
+    pairs, on all host threads (the FP64 oracle's whole-job time where oracle/_ref is not built).
+    The FP64 oracle runs the whole job once, and the timed job's offsets are checked against it
+    pair by pair (oracle.parity.compare; the same worker reruns the job with diagnostics and
+    surfaces, and its offsets must equal the timed ones bit for bit)."""
     import torch
 
     from oracle import parity
     from ampcor_b200.worker import DIAG_DTYPE
+
+    from oracle import ref as refcpu
 
     dev = ref.device
     P = w.pairs
@@ -454,12 +495,19 @@ def cpu_leg(w, worker, ref, tgt, ulhc, timed_offsets):
     orc = parity.oracle_run(w.ref, w.tgt, w.ulhc, w.chip, w.window, w.refine_factor,
                             w.refine_margin, w.zoom_factor, threads=threads)
     dt = orc["adjust_seconds"]
-    cpu = {"value": P / dt, "unit": UNIT, "cores": threads, "kind": "port",
-           "sample": (f"the whole job ({P} pairs) through the FP64 restatement of the full "
-                      f"reference pipeline (oracle/oracle.c: coarse NCC, nudge, FFT refinement, "
-                      f"refined NCC, zoom, offsets), OpenMP over pairs, {dt:.1f} s on {threads} "
-                      f"threads")}
+    if refcpu.available():
+        with refcpu.Rasters(w.ref, w.tgt) as rasters:
+            rate, n, rdt = reference_rate(w, rasters, 15.0, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": f"{REFERENCE_SAMPLE}: {n} random pairs of the workload, {rdt:.1f} s on {threads} threads"}
+    else:
+        cpu = {"value": P / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"the whole job ({P} pairs) through the FP64 restatement of the full "
+                          f"reference pipeline (oracle/oracle.c: coarse NCC, nudge, FFT refinement, "
+                          f"refined NCC, zoom, offsets), OpenMP over pairs, {dt:.1f} s on {threads} "
+                          f"threads")}
     rep = parity.summary(parity.compare(orc, gpu_off, gpu_diag, cs_h, rs_h))
+    rep["oracle_pairs_per_s"] = P / dt
     rep["rerun_equals_timed_offsets"] = same_as_timed
     rep["rule"] = ("every pair against the FP64 oracle: cells equal (offsets then bit-exact) "
                    "unless the pair's own measured surface error explains a near-tie, counted "

@@ -64,7 +64,7 @@ def load():
         lib = ctypes.CDLL(LIB)
         lib.oracle_coarse_cpu.restype = None
         lib.oracle_coarse_cpu.argtypes = [POINTER(Src), c_longlong, c_int, c_int, c_void_p,
-                                          c_void_p, c_void_p, c_int]
+                                          c_void_p, c_void_p, c_int, c_int]
         lib.oracle_adjust.restype = None
         lib.oracle_adjust.argtypes = [POINTER(Src), c_longlong, POINTER(Geom), c_void_p,
                                       c_void_p, c_void_p, c_void_p, c_int]
@@ -113,8 +113,13 @@ class Sources:
                        self.tgt.ctypes.data, self.tgt_off.ctypes.data, self.tgt.shape[1])
 
 
-def coarse_cpu(ref, tgt, ulhc, R, W, surfaces=False, threads=None):
-    """Reference CPU coarse correlator.  Returns (argmax (P,2) int32, gap (P,), [surfaces])."""
+def coarse_cpu(ref, tgt, ulhc, R, W, surfaces=False, threads=None, as_built=False):
+    """Reference CPU coarse correlator.  Returns (argmax (P,2) int32, gap (P,), [surfaces]).
+
+    ``as_built=False`` (the default, and the integer-offset gate) centres each placement on its
+    window box mean, as the reference intends and its CUDA worker does; ``as_built=True`` repeats
+    the arithmetic of the reference's CPU code as written, whose summed-area table is built over
+    an empty grid (lib/libampcor/correlators/Sequential.cc:48), so no mean is taken off."""
     s = Sources(ref, tgt, ulhc)
     C = W - R + 1
     arg = np.zeros((s.pairs, 2), np.int32)
@@ -122,7 +127,7 @@ def coarse_cpu(ref, tgt, ulhc, R, W, surfaces=False, threads=None):
     cor = np.zeros((s.pairs, C, C), np.float64) if surfaces else None
     load().oracle_coarse_cpu(ctypes.byref(s.src), s.pairs, R, W,
                              cor.ctypes.data if surfaces else None, arg.ctypes.data,
-                             gap.ctypes.data, _threads(threads))
+                             gap.ctypes.data, _threads(threads), int(bool(as_built)))
     return (arg, gap, cor) if surfaces else (arg, gap)
 
 

@@ -302,9 +302,18 @@ void oracle_zoom(const double *G, int Cf, int z, const double *U, int use_abs, d
  * the raw chip, per anchor tAvg = SAT box / R^2, num = sum a_r (t - tAvg),
  * tVar = sum (t - tAvg)^2, cor = num / sqrt(rVar * tVar).
  * cor (P x C^2, may be NULL), argmax (2P: row, col), gap (P, may be NULL): top-2 gap.
+ *
+ * as_built selects where tAvg comes from.  0: the window's own box mean (the summed-area table
+ * of the window amplitudes, the intent, and what the reference's CUDA worker computes:
+ * sat.cu:81-149, tgtStats.cu:88-168).  1: the arithmetic of the reference's CPU code as it is
+ * written: Sequential.cc:48 builds its table as `sat_type sat(tgt.layout())`, i.e. over a new
+ * grid of the window's layout rather than over the window, so with that storage zero every box
+ * sum and tAvg are 0 and cor is the uncentred sum a_r t / sqrt(sum a_r^2 sum t^2); the sums then
+ * run in the reference's order, one term at a time (no vectorised reduction), so that the values
+ * match the compiled reference (oracle/_ref) to the last bit.
  */
 void oracle_coarse_cpu(const oracle_src *src, i64 pairs, int R, int W,
-                       double *cor, int *argmax, double *gap, int threads)
+                       double *cor, int *argmax, double *gap, int threads, int as_built)
 {
     const int C = W - R + 1;
 #ifdef _OPENMP
@@ -332,16 +341,26 @@ void oracle_coarse_cpu(const oracle_src *src, i64 pairs, int R, int W,
             const double cells = (double)R * R;
             for (int u = 0; u < C; ++u)
                 for (int v = 0; v < C; ++v) {
-                    const double tAvg = oracle_box(sat, W, u, v, u + R, v + R) / cells;
                     double num = 0.0, tVar = 0.0;
-                    for (int i = 0; i < R; ++i)
+                    if (as_built) {
+                        for (int i = 0; i < R; ++i)
+                            for (int j = 0; j < R; ++j) {
+                                const double rv = ref[(i64)i * R + j];
+                                const double tv = tgt[(i64)(u + i) * W + v + j];
+                                num += rv * tv;
+                                tVar += tv * tv;
+                            }
+                    } else {
+                        const double tAvg = oracle_box(sat, W, u, v, u + R, v + R) / cells;
+                        for (int i = 0; i < R; ++i)
 #pragma omp simd reduction(+ : num, tVar)
-                        for (int j = 0; j < R; ++j) {
-                            const double rv = ref[(i64)i * R + j];
-                            const double tv = tgt[(i64)(u + i) * W + v + j] - tAvg;
-                            num += rv * tv;
-                            tVar += tv * tv;
-                        }
+                            for (int j = 0; j < R; ++j) {
+                                const double rv = ref[(i64)i * R + j];
+                                const double tv = tgt[(i64)(u + i) * W + v + j] - tAvg;
+                                num += rv * tv;
+                                tVar += tv * tv;
+                            }
+                    }
                     g[(i64)u * C + v] = num / sqrt(rVar * tVar);
                 }
             const int k = oracle_argmax_first(g, (i64)C * C);
