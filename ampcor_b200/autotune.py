@@ -76,7 +76,10 @@ def tune(worker, ref, tgt, ulhc, forms=("spectral", "tensor", "plain"), chunks=D
                 continue
             if worker.form != form:
                 continue
-            worker.correlate(ref, tgt, ulhc, offsets=out, synchronize=True)
+            try:
+                worker.correlate(ref, tgt, ulhc, offsets=out, synchronize=True)
+            except Error:
+                continue  # e.g. the chunk's scratch does not fit beside the caller's data
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()

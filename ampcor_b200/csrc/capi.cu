@@ -254,6 +254,67 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     return true;
 }
 
+// A stage of the spectral form whose window is too large for one tile: the chip splits into nb x nb
+// square blocks of side B (B divides R), each block's sub-window (B + C - 1 samples a side) one
+// tile; the largest B whose tile fits is taken.  `full` describes the whole stage for the
+// reduction.
+struct SpecBlocks {
+    bool on = false;
+    int B = 0, nb = 0, K = 0;
+    SpecGeom tile{};
+    SpecGeom full{};
+};
+
+bool plan_spec_tile(int B, int S, int C, SpecGeom& g)
+{
+    std::memset(&g, 0, sizeof(g));
+    g.R = B;
+    g.W = S;
+    g.C = C;
+    g.N = spec_next_length(S);
+    if (g.N == 0 || !spec_radices(g.N, g.N1, g.N2)) return false;
+    auto up = [](long x, long a) { return (x + a - 1) / a * a; };
+    g.RS = g.N + 1;
+    long off = up((long)g.N * g.RS * 8, 16);
+    g.off_z = 0;
+    g.off_tw = (int)off;
+    off = up(off + (long)g.N * 8, 16);
+    g.off_neg = (int)off;
+    off = up(off + (long)g.N * 4, 16);
+    g.off_red = (int)off;
+    off += 256;
+    g.smem_bytes = (int)off;
+    return off <= 227L * 1024;
+}
+
+bool plan_spec_blocked(int R, int W, SpecBlocks& b, std::string& err)
+{
+    b = SpecBlocks{};
+    const int C = W - R + 1;
+    int tile_smem = 0;
+    if (R < 1 || C < 1 || spec_tile_stats_rows(W, C, tile_smem) == 0 || spec_reduce_smem(C) > 227 * 1024) {
+        err = "the blocked spectral form needs a window of at most 512 samples and at most 165 "
+              "placements per axis";
+        return false;
+    }
+    for (int B = R; B >= 1; --B) {
+        if (R % B) continue;
+        const int nb = R / B;
+        if (nb * nb > 64) break;
+        if (!plan_spec_tile(B, B + C - 1, C, b.tile)) continue;
+        b.on = true;
+        b.B = B;
+        b.nb = nb;
+        b.K = nb * nb;
+        b.full.R = R;
+        b.full.W = W;
+        b.full.C = C;
+        return true;
+    }
+    err = "no block of the chip fits the spectral form (the search margin is too large)";
+    return false;
+}
+
 // the tensor-core zoom: operand planes, accumulator parts and row tiles; false when Zm does not fit
 // (more than 512 accumulator columns or more shared memory than a CTA has)
 bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
@@ -436,9 +497,22 @@ struct ampcor_handle {
     float* d_zoom_uhl = nullptr;
     float* d_tw_c = nullptr;
     float* d_tw_f = nullptr;
-    // refinement by zero-padded FFT (spectral form): twiddles of R, f R, E and f E, in that order
+    // refinement by zero-padded FFT (spectral form): twiddles of R, f R, E and f E, in that order;
+    // tiles too large to stage whole go through a per-pair buffer (d_upy, chunk x upy_len)
     bool refine_fft = false;
     float* d_tw_refine = nullptr;
+    bool refine_big = false;
+    float2* d_upy = nullptr;
+    long long upy_len = 0;
+    // blocked spectral stages (coarse, fine): chip statistics, placement statistics, partial
+    // numerators and their scalars, all per chunk
+    SpecBlocks bc{}, bf{};
+    ChipStat* d_cstat = nullptr;
+    float* d_inv_blk = nullptr;
+    float* d_part = nullptr;
+    double* d_scal = nullptr;
+    // forms the geometry allows
+    bool plain_ok = false, tensor_ok = false, spectral_ok = false;
     // amplitude rasters of the spectral form (reference and secondary, one allocation), and the
     // box statistics of the secondary raster (FP64 column sums, 1/sigma of every box)
     float* d_amp = nullptr;
@@ -541,6 +615,35 @@ size_t default_chunk()
     return 148 * 4;
 }
 
+void free_chunk_scratch(ampcor_handle* h)
+{
+    cudaFree(h->d_refined);
+    cudaFree(h->d_inv_c);
+    cudaFree(h->d_inv_f);
+    cudaFree(h->d_gam);
+    cudaFree(h->d_cstat);
+    cudaFree(h->d_inv_blk);
+    cudaFree(h->d_part);
+    cudaFree(h->d_scal);
+    cudaFree(h->d_upy);
+    h->d_refined = nullptr;
+    h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
+    h->d_cstat = nullptr;
+    h->d_inv_blk = nullptr;
+    h->d_part = nullptr;
+    h->d_scal = nullptr;
+    h->d_upy = nullptr;
+}
+
+// a failed chunk-scratch allocation releases what was allocated, so that the next call starts
+// over, and clears the runtime's record of the failure (it is reported here, not by a later launch)
+int scratch_fail(ampcor_handle* h, const std::string& what)
+{
+    free_chunk_scratch(h);
+    cudaGetLastError();
+    return fail(h, AMPCOR_E_NOMEM, what);
+}
+
 int ensure_refined(ampcor_handle* h)
 {
     if (h->d_refined) return AMPCOR_OK;
@@ -549,7 +652,7 @@ int ensure_refined(ampcor_handle* h)
     cudaError_t e = cudaMalloc(&h->d_refined, h->chunk * h->refined_stride * sizeof(float));
     if (e != cudaSuccess) {
         h->d_refined = nullptr;
-        return fail(h, AMPCOR_E_NOMEM, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
+        return scratch_fail(h, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
     }
     const size_t n = h->chunk;
     // per-pair placement statistics: only the tensor-core form stages them in memory (the
@@ -557,11 +660,26 @@ int ensure_refined(ampcor_handle* h)
     if (h->form == kFormTensor &&
         (cudaMalloc(&h->d_inv_c, n * h->C * h->C * sizeof(float)) != cudaSuccess ||
          cudaMalloc(&h->d_inv_f, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess))
-        return fail(h, AMPCOR_E_NOMEM, "allocating placement statistics scratch");
+        return scratch_fail(h, "allocating placement statistics scratch");
     if (h->form != kFormPlain && cudaMalloc(&h->d_gam, n * h->Cf * h->Cf * sizeof(float)) != cudaSuccess)
-        return fail(h, AMPCOR_E_NOMEM, "allocating refined-surface scratch");
+        return scratch_fail(h, "allocating refined-surface scratch");
+    if (h->form == kFormSpectral && (h->bc.on || h->bf.on)) {
+        const size_t K = (size_t)std::max(h->bc.on ? h->bc.K : 0, h->bf.on ? h->bf.K : 0);
+        const size_t parts = std::max(h->bc.on ? (size_t)h->bc.K * h->C * h->C : 0,
+                                      h->bf.on ? (size_t)h->bf.K * h->Cf * h->Cf : 0);
+        const size_t cells = std::max(h->bc.on ? (size_t)h->C * h->C : 0, h->bf.on ? (size_t)h->Cf * h->Cf : 0);
+        if (cudaMalloc(&h->d_cstat, n * sizeof(ChipStat)) != cudaSuccess ||
+            cudaMalloc(&h->d_inv_blk, n * cells * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&h->d_part, n * parts * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&h->d_scal, n * K * 2 * sizeof(double)) != cudaSuccess)
+            return scratch_fail(h, "allocating blocked-correlation scratch");
+    }
+    if (h->form == kFormSpectral && h->refine_big &&
+        cudaMalloc(&h->d_upy, n * (size_t)h->upy_len * sizeof(float2)) != cudaSuccess)
+        return scratch_fail(h, "allocating refinement scratch");
     return AMPCOR_OK;
 }
+
 
 int ensure_fine_out(ampcor_handle* h, size_t pairs)
 {
@@ -789,21 +907,44 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
     for (long long c0 = p0; c0 < p1; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, p1 - c0);
         cudaEvent_t b = mark(h, st);
-        CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
-                          reinterpret_cast<const float2*>(h->d_tw_c),
-                          SpecOut{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces}),
-           "launching the spectral coarse correlation");
+        const SpecOut co{0, h->m, h->d_coarse, h->d_coarse_peak, nullptr, nullptr, coarse_surfaces};
+        if (h->bc.on) {
+            InvSource ic = r.inv_c;
+            CK(h, launch_spec_chip_stats(n, st, cs, c0, n, src.ref_off, h->R, h->d_cstat),
+               "launching the chip statistics");
+            int kernels = 1;
+            if (!ic.base) {
+                CK(h, launch_spec_tile_stats(n, st, cs, c0, n, src.ref_off, h->R, h->W, h->d_inv_blk),
+                   "launching the placement statistics");
+                ic = InvSource{h->d_inv_blk, nullptr, 0};
+                ++kernels;
+            }
+            cudaEvent_t b2 = mark(h, st);
+            keep(h, 3, b, b2, kernels);
+            b = b2;
+            CK(h, launch_spec_block(h->bc.tile, h->bc.nb, n * (unsigned)h->bc.K, st, cs, c0, n, src.ref_off,
+                                    h->d_cstat, reinterpret_cast<const float2*>(h->d_tw_c), h->d_part, h->d_scal),
+               "launching the blocked coarse correlation");
+            CK(h, launch_spec_reduce(h->bc.full, h->bc.K, n, st, cs, c0, n, src.ref_off, h->d_cstat, ic,
+                                     h->d_part, h->d_scal, co),
+               "launching the coarse reduction");
+        } else {
+            CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
+                              reinterpret_cast<const float2*>(h->d_tw_c), co),
+               "launching the spectral coarse correlation");
+        }
         cudaEvent_t c = mark(h, st);
-        keep(h, 0, b, c);
+        keep(h, 0, b, c, h->bc.on ? 2 : 1);
         if (h->refine_fft) {
             const float2* tw = reinterpret_cast<const float2*>(h->d_tw_refine);
             CK(h, launch_spec_refine(h->R, n, st, src.ref_base, src.ref_off, src.ref_stride, nullptr, c0,
                                      n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0,
-                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0),
+                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy),
                "launching the chip refinement");
             CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
                                      c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
-                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf, (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0),
+                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf,
+                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy),
                "launching the window refinement");
         } else {
             refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
@@ -813,12 +954,28 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
         }
         cudaEvent_t e = mark(h, st);
         keep(h, 1, c, e, h->refine_fft ? 2 : 1);
-        CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
-                          reinterpret_cast<const float2*>(h->d_tw_f),
-                          SpecOut{1, 0, nullptr, nullptr, h->d_fine_out, h->d_gam, refined_surfaces}),
-           "launching the spectral fine correlation");
+        const SpecOut fo{1, 0, nullptr, nullptr, h->d_fine_out, h->d_gam, refined_surfaces};
+        if (h->bf.on) {
+            CK(h, launch_spec_chip_stats(n, st, fs, c0, n, src.ref_off, h->Rf, h->d_cstat),
+               "launching the refined chip statistics");
+            CK(h, launch_spec_tile_stats(n, st, fs, c0, n, src.ref_off, h->Rf, h->Wf, h->d_inv_blk),
+               "launching the refined placement statistics");
+            cudaEvent_t e2 = mark(h, st);
+            keep(h, 4, e, e2, 2);
+            e = e2;
+            CK(h, launch_spec_block(h->bf.tile, h->bf.nb, n * (unsigned)h->bf.K, st, fs, c0, n, src.ref_off,
+                                    h->d_cstat, reinterpret_cast<const float2*>(h->d_tw_f), h->d_part, h->d_scal),
+               "launching the blocked fine correlation");
+            CK(h, launch_spec_reduce(h->bf.full, h->bf.K, n, st, fs, c0, n, src.ref_off, h->d_cstat,
+                                     InvSource{h->d_inv_blk, nullptr, 0}, h->d_part, h->d_scal, fo),
+               "launching the fine reduction");
+        } else {
+            CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
+                              reinterpret_cast<const float2*>(h->d_tw_f), fo),
+               "launching the spectral fine correlation");
+        }
         cudaEvent_t f = mark(h, st);
-        keep(h, 2, e, f);
+        keep(h, 2, e, f, h->bf.on ? 2 : 1);
         if ((rc = launch_zoom(h, c0, n, src, offsets, diag, st))) return rc;
         keep(h, 5, f, mark(h, st));
     }
@@ -909,33 +1066,59 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
             break;
         }
     h->zg.taps_len = 2 * h->Cf + 32;
-    if (!plan_ncc(h->R, h->W, 0, 0, h->gc, err) ||
-        !plan_ncc(h->Rf, h->Wf, h->Cf * h->Z, h->z * h->zg.taps_len, h->gf, err) ||
-        !plan_interp(h->R, h->f, h->ic, err) || !plan_interp(h->E, h->f, h->iw, err)) {
-        delete h;
-        return create_fail(AMPCOR_E_SHAPE, err);
-    }
-    h->refine_smem = std::max(h->ic.smem_bytes, h->iw.smem_bytes);
-    // the spectral form where the geometry allows it, else the tensor-core form, else the plain
-    // form; AMPCOR_FLAG_PLAIN_FP32 (or AMPCOR_FORM=plain|tensor|spectral) chooses
+    // the forms this geometry allows: the plain form (direct FP32 sums, whole tiles in shared
+    // memory, refinement by interpolation taps), the tensor-core form (the same refinement) and
+    // the spectral form (each correlation stage in one tile, or in chip blocks where the window
+    // is too large; refinement by zero-padded FFT, or by taps where no FFT length is compiled)
     {
+        std::string perr, terr, serr;
+        const bool interp_ok = plan_interp(h->R, h->f, h->ic, perr) && plan_interp(h->E, h->f, h->iw, perr);
+        h->plain_ok = plan_ncc(h->R, h->W, 0, 0, h->gc, perr) &&
+                      plan_ncc(h->Rf, h->Wf, h->Cf * h->Z, h->z * h->zg.taps_len, h->gf, perr) && interp_ok;
+        h->tensor_ok = h->plain_ok && plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
+        int sm_c = 0, sm_w = 0;
+        const bool small_c = spec_refine_supported(h->R, h->f, sm_c), small_w = spec_refine_supported(h->E, h->f, sm_w);
+        const bool big_c = !small_c && spec_refine_big_supported(h->R, h->f, sm_c);
+        const bool big_w = !small_w && spec_refine_big_supported(h->E, h->f, sm_w);
+        h->refine_fft = (small_c || big_c) && (small_w || big_w) &&
+                        !(std::getenv("AMPCOR_REFINE_TAPS") && interp_ok);
+        h->refine_big = h->refine_fft && (big_c || big_w);
+        h->upy_len = std::max((long long)h->R * h->Rf, (long long)h->E * h->Wf);
+        const bool direct_c = plan_spec(h->R, h->W, h->spc, serr);
+        const bool coarse_ok = direct_c || plan_spec_blocked(h->R, h->W, h->bc, serr);
+        const bool direct_f = coarse_ok && plan_spec(h->Rf, h->Wf, h->spf, serr);
+        const bool fine_ok = coarse_ok && (direct_f || plan_spec_blocked(h->Rf, h->Wf, h->bf, serr));
+        h->spectral_ok = fine_ok && (h->refine_fft || interp_ok);
+        if (direct_c || !h->spectral_ok) h->bc = SpecBlocks{};
+        if (direct_f || !h->spectral_ok) h->bf = SpecBlocks{};
+        if (!h->spectral_ok && serr.empty()) serr = "no refinement of these tiles is compiled";
+        if (!h->plain_ok && !h->spectral_ok) {
+            delete h;
+            return create_fail(AMPCOR_E_SHAPE, perr + "; " + serr);
+        }
+        h->refine_smem = std::max(h->ic.smem_bytes, h->iw.smem_bytes);
+        // the spectral form where the geometry allows it, else the tensor-core form, else the plain
+        // form; AMPCOR_FLAG_PLAIN_FP32 (or AMPCOR_FORM=plain|tensor|spectral) chooses among those
+        // allowed
         const char* env = std::getenv("AMPCOR_FORM");
-        std::string terr;
-        const bool spec_ok = plan_spec(h->R, h->W, h->spc, terr) && plan_spec(h->Rf, h->Wf, h->spf, terr);
-        const bool tc_ok = plan_tc(h->R, h->W, 8, h->tcc, terr) && plan_tc(h->Rf, h->Wf, 4, h->tcf, terr);
-        h->form = spec_ok ? kFormSpectral : tc_ok ? kFormTensor : kFormPlain;
+        h->form = h->spectral_ok ? kFormSpectral : h->tensor_ok ? kFormTensor : kFormPlain;
+        if ((p->flags & AMPCOR_FLAG_PLAIN_FP32) && !h->plain_ok) {
+            delete h;
+            return create_fail(AMPCOR_E_SHAPE, "this geometry has no plain FP32 form: " + perr);
+        }
         if (p->flags & AMPCOR_FLAG_PLAIN_FP32) h->form = kFormPlain;
-        if (env && std::strcmp(env, "plain") == 0) h->form = kFormPlain;
-        if (env && std::strcmp(env, "tensor") == 0 && tc_ok) h->form = kFormTensor;
-        if (env && std::strcmp(env, "spectral") == 0 && spec_ok) h->form = kFormSpectral;
+        if (env && std::strcmp(env, "plain") == 0 && h->plain_ok) h->form = kFormPlain;
+        if (env && std::strcmp(env, "tensor") == 0 && h->tensor_ok) h->form = kFormTensor;
+        if (env && std::strcmp(env, "spectral") == 0 && h->spectral_ok) h->form = kFormSpectral;
         h->gsc = stats_layout(h->gc);
         h->gsf = stats_layout(h->gf);
         const int Zp = (h->Z + 7) & ~7;
         h->zoom_smem = (round4(h->Cf * h->Cf) + 2 * h->Cf * Zp + 64) * 4;
         h->zoom_tc = plan_zoom_tc(h->Cf, h->z, h->ztc) && !std::getenv("AMPCOR_ZOOM_FP32");
-        int sm_c = 0, sm_w = 0;
-        h->refine_fft = spec_refine_supported(h->R, h->f, sm_c) && spec_refine_supported(h->E, h->f, sm_w) &&
-                        !std::getenv("AMPCOR_REFINE_TAPS");
+        if (!h->zoom_tc && h->zoom_smem > 227 * 1024) {
+            delete h;
+            return create_fail(AMPCOR_E_SHAPE, "the zoomed surface is too large for this build");
+        }
     }
 
     cudaError_t e = cudaSetDevice(p->device);
@@ -996,8 +1179,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     };
     if ((e = upload(h->d_chip_taps, ct)) != cudaSuccess || (e = upload(h->d_win_taps, wt)) != cudaSuccess ||
         (e = upload(h->d_zoom_taps, zt)) != cudaSuccess || (e = upload(h->d_zoom_ut, zut)) != cudaSuccess ||
-        (e = upload(h->d_tw_c, spec_twiddle_table(std::max(h->spc.N, 1)))) != cudaSuccess ||
-        (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->spf.N, 1)))) != cudaSuccess ||
+        (e = upload(h->d_tw_c, spec_twiddle_table(std::max(h->bc.on ? h->bc.tile.N : h->spc.N, 1)))) != cudaSuccess ||
+        (e = upload(h->d_tw_f, spec_twiddle_table(std::max(h->bf.on ? h->bf.tile.N : h->spf.N, 1)))) != cudaSuccess ||
         (h->zoom_tc && (e = upload(h->d_zoom_uhl, zoom_u_planes(h->ztc))) != cudaSuccess))
         return cuda_create_fail(e, "uploading interpolation taps");
     if (h->refine_fft) {
@@ -1053,6 +1236,11 @@ int ampcor_destroy(ampcor_handle* h)
     cudaFree(h->d_vsum);
     cudaFree(h->d_inv_raster);
     cudaFree(h->d_tc_err);
+    cudaFree(h->d_cstat);
+    cudaFree(h->d_inv_blk);
+    cudaFree(h->d_part);
+    cudaFree(h->d_scal);
+    cudaFree(h->d_upy);
     drop_marks(h);
     if (h->h_arena) cudaFreeHost(h->h_arena);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
@@ -1392,35 +1580,23 @@ int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
     CK(h, cudaSetDevice(h->prm.device), "cudaSetDevice");
     CK(h, cudaStreamSynchronize(h->stream), "waiting for the worker");
     if (form == kFormTensor) {
-        std::string terr;
-        if (!plan_tc(h->R, h->W, 8, h->tcc, terr) || !plan_tc(h->Rf, h->Wf, 4, h->tcf, terr))
-            return fail(h, AMPCOR_E_SHAPE, "this geometry has no tensor-core form: " + terr);
+        if (!h->tensor_ok) return fail(h, AMPCOR_E_SHAPE, "this geometry has no tensor-core form");
     } else if (form == kFormSpectral) {
-        std::string terr;
-        if (!plan_spec(h->R, h->W, h->spc, terr) || !plan_spec(h->Rf, h->Wf, h->spf, terr))
-            return fail(h, AMPCOR_E_SHAPE, "this geometry has no spectral form: " + terr);
-    } else if (form != kFormPlain && form != -1) {
+        if (!h->spectral_ok) return fail(h, AMPCOR_E_SHAPE, "this geometry has no spectral form");
+    } else if (form == kFormPlain) {
+        if (!h->plain_ok) return fail(h, AMPCOR_E_SHAPE, "this geometry has no plain FP32 form");
+    } else if (form != -1) {
         return fail(h, AMPCOR_E_ARG, "form must be -1, 0, 1 or 2");
     }
     const bool switching = form != -1 && form != h->form;
     if (form != -1) h->form = form;
     if (chunk && chunk != h->chunk) {
         // the chunk scratch is sized on first use
-        cudaFree(h->d_refined);
-        cudaFree(h->d_inv_c);
-        cudaFree(h->d_inv_f);
-        cudaFree(h->d_gam);
-        h->d_refined = nullptr;
-        h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
+        free_chunk_scratch(h);
         h->chunk_override = (size_t)chunk;
     } else if (switching && h->d_refined) {
         // a form switch needs the chunk scratch of the new form
-        cudaFree(h->d_refined);
-        cudaFree(h->d_inv_c);
-        cudaFree(h->d_inv_f);
-        cudaFree(h->d_gam);
-        h->d_refined = nullptr;
-        h->d_inv_c = h->d_inv_f = h->d_gam = nullptr;
+        free_chunk_scratch(h);
     }
     return AMPCOR_OK;
 }

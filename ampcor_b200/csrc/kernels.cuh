@@ -264,6 +264,12 @@ struct InvSource {
     long long stride;
 };
 
+// per-pair chip statistics of a blocked spectral stage: the chip's FP64 mean and 1/|r - mean|
+struct ChipStat {
+    double mean;
+    double inv_sigma;
+};
+
 // the transform lengths that are compiled, with their radices
 bool spec_radices(int n, int& n1, int& n2);
 int spec_next_length(int w);
@@ -271,11 +277,33 @@ int spec_next_length(int w);
 cudaError_t spec_set_smem_limits();
 // refinement by zero-padded FFT for an N x N tile and factor f, when compiled (smem: its bytes)
 bool spec_refine_supported(int n, int f, int& smem);
+// refinement of tiles too large for one CTA's shared memory (N in 96 .. 160, f = 2): rows and
+// columns in strips through a per-pair buffer of N x 2N complex samples (ybuf, blocks of them)
+bool spec_refine_big_supported(int n, int f, int& smem);
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
-                               long long refined_stride, long long out_off, int deramp);
+                               long long refined_stride, long long out_off, int deramp,
+                               float2* ybuf);
+
+// blocked spectral correlation (windows too large for one tile; see spectral.cu): per chunk of
+// pairs the chip statistics, the placement statistics when no raster gives them, the partial
+// numerators of every (pair, chip block) and their per-pair reduction to the stage's outputs
+cudaError_t launch_spec_chip_stats(unsigned blocks, cudaStream_t st, SpecSource src, long long pair0,
+                                   long long pairs, const long long* valid, int R, ChipStat* out);
+int spec_tile_stats_rows(int W, int C, int& smem);
+cudaError_t launch_spec_tile_stats(unsigned blocks, cudaStream_t st, SpecSource src, long long pair0,
+                                   long long pairs, const long long* valid, int R, int W, float* inv);
+cudaError_t launch_spec_block(const SpecGeom& tile, int nb, unsigned blocks, cudaStream_t st,
+                              SpecSource src, long long pair0, long long pairs,
+                              const long long* valid, const ChipStat* cstat, const float2* tw,
+                              float* part, double* scal);
+int spec_reduce_smem(int C);
+cudaError_t launch_spec_reduce(const SpecGeom& full, int K, unsigned blocks, cudaStream_t st,
+                               SpecSource src, long long pair0, long long pairs,
+                               const long long* valid, const ChipStat* cstat, InvSource inv,
+                               const float* part, const double* scal, SpecOut out);
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
                         long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out);

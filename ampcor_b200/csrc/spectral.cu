@@ -616,6 +616,427 @@ spec_refine_kernel(const float2* base, const long long* off, long long stride,
     X(144, 12, 12)             \
     X(160, 10, 16)
 
+// ------------------------------------------------------------------------------------------
+// blocked spectral correlation: tiles beyond one CTA's shared memory
+// ------------------------------------------------------------------------------------------
+//
+// The numerator surface is a sum over the chip's pixels, so it splits over square blocks of the
+// chip: block k (rows [i0, i0 + B), columns [j0, j0 + B)) meets the sub-window of rows
+// [i0, i0 + B + C - 1), columns [j0, j0 + B + C - 1), and its placements are those of the whole
+// window.  spec_block_kernel runs the in-shared-memory FFT correlation of one block (one CTA per
+// pair and block) and writes its partial numerators; spec_reduce_kernel sums a pair's partials in
+// a fixed order, normalises them, bounds the transform error and takes the first maximum, as
+// spec_kernel does for a tile that fits.  The chip is centred on the whole chip's mean
+// (spec_chip_stats_kernel), each sub-window on its own mean s_k: the block then computes
+// sum c (t - s_k), and the pair's numerator is the sum over blocks plus sum_k s_k sum_k c, c the
+// centred chip values the block placed in its tile.
+
+// one CTA of 256 threads per pair: FP64 mean and 1/|r - mean| of the R x R chip
+__global__ void __launch_bounds__(256)
+spec_chip_stats_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, int R,
+                       ChipStat* out)
+{
+    __shared__ double red[16];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (valid[p] < 0) {
+        if (tid == 0) out[blockIdx.x] = ChipStat{0.0, 0.0};
+        return;
+    }
+    const float* chip = spec_chip(src, pair0, blockIdx.x);
+    const long long cs = src.chip_stride;
+    double s1 = 0.0, s2 = 0.0;
+    for (int y = warp; y < R; y += 8)
+        for (int x = lane; x < R; x += 32) {
+            const double v = __ldg(chip + y * cs + x);
+            s1 += v;
+            s2 += v * v;
+        }
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if (lane == 0) {
+        red[2 * warp] = s1;
+        red[2 * warp + 1] = s2;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            a += red[2 * w];
+            b += red[2 * w + 1];
+        }
+        const double cells = (double)R * (double)R;
+        const double mean = a / cells;
+        const double ss = b - cells * mean * mean;
+        out[blockIdx.x] = ChipStat{mean, ss > 0.0 ? 1.0 / sqrt(ss) : 0.0};
+    }
+}
+
+// 1/sigma of every placement box of a window read straight from global memory (windows larger
+// than a CTA stages): FP64 column sums sliding down the window, FP64 prefix sums along the rows,
+// SR placement rows at a time (window_stats_xs); inv: C^2 floats per chunk-local pair.  W <= kThreads.
+__global__ void __launch_bounds__(kThreads, 2)
+spec_tile_stats_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, int R, int W,
+                       int SR, float* inv)
+{
+    extern __shared__ __align__(16) double tsm[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    if (valid[p] < 0) return;
+    const int C = W - R + 1;
+    window_stats_xs<1>(spec_win(src, pair0, blockIdx.x), (int)src.win_stride, W, R, C, SR,
+                       inv + (long long)blockIdx.x * C * C, tsm);
+}
+
+// The partial numerators of one chip block of one pair (CTA b K + k): g is the tile of a block
+// (g.R = B, g.W = B + C - 1, g.C = C), nb blocks per axis.  part: C^2 floats per (pair, block),
+// already scaled; scal: two doubles per (pair, block), s_k sum_k c and |c| |t - s_k|.
+template <int N1, int N2>
+__global__ void __launch_bounds__(kThreads, 1)
+spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
+                  int nb, const ChipStat* cstat, const float2* tw_g, float* part, double* scal)
+{
+    extern __shared__ __align__(16) unsigned char ssm[];
+    const int K = nb * nb;
+    const int b = blockIdx.x / K, k = blockIdx.x - b * K;
+    if (b >= pairs) return;
+    const long long p = pair0 + b;
+    if (valid[p] < 0) return;
+    constexpr int N = N1 * N2;
+    constexpr int RS = N + 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int B = g.R, S = g.W, C = g.C;
+    const int i0 = (k / nb) * B, j0 = (k - (k / nb) * nb) * B;
+    float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
+    float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
+    int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
+    double* red = reinterpret_cast<double*>(ssm + g.off_red);
+    float* Zf = reinterpret_cast<float*>(Z);
+    const long long cs = src.chip_stride, ws = src.win_stride;
+    const float* chip = spec_chip(src, pair0, b) + i0 * cs + j0;
+    const float* win = spec_win(src, pair0, b) + i0 * ws + j0;
+    const ChipStat cst = cstat[b];
+    const float mc_hi = (float)cst.mean, mc_lo = (float)(cst.mean - (double)mc_hi);
+
+    // the block of the chip, centred on the whole chip's mean, to registers; the sub-window to the
+    // tile's real parts by asynchronous copies, zeros around it
+    constexpr int JN = (N + kWarps - 1) / kWarps, IN = (N + 31) / 32;
+    float cr[JN][IN];
+#pragma unroll
+    for (int j = 0; j < JN; ++j)
+#pragma unroll
+        for (int i = 0; i < IN; ++i) {
+            const int y = warp + kWarps * j, x = lane + 32 * i;
+            cr[j][i] = y < B && x < B ? (__ldg(chip + y * cs + x) - mc_hi) - mc_lo : 0.0f;
+        }
+    for (int y = warp; y < N; y += kWarps) {
+        float* zr = Zf + 2 * y * RS;
+        for (int x = lane; x < N; x += 32) {
+            if (y < S && x < S)
+                cp_async4(zr + 2 * x, win + y * ws + x);
+            else
+                zr[2 * x] = 0.0f;
+        }
+    }
+    for (int q = tid; q < N; q += kThreads) {
+        tw[q] = __ldg(tw_g + q);
+        neg[q] = fft::neg_pos<N1, N2>(q);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // FP64 sums of the centred chip block (its sum and sum of squares) and of the sub-window
+    double a0 = 0.0, a1 = 0.0, a2, a3;
+    {
+        float sw = 0.0f, sw2 = 0.0f;
+        for (int y = warp; y < S; y += kWarps) {
+            const float2* zr = Z + y * RS;
+            for (int x = lane; x < S; x += 32) {
+                const float t = zr[x].x;
+                sw += t;
+                sw2 = fmaf(t, t, sw2);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int i = 0; i < IN; ++i) {
+                const double c = cr[j][i];
+                a0 += c;
+                a1 += c * c;
+            }
+        a2 = sw;
+        a3 = sw2;
+        block_sum2(a0, a1, red);
+        block_sum2(a2, a3, red);
+    }
+    const double cells_w = (double)S * (double)S;
+    const double mean_w = a2 / cells_w;
+    const double st = fmax(a3 - cells_w * mean_w * mean_w, 0.0);
+    const fft::Centre centre{(float)mean_w, S};
+#pragma unroll
+    for (int j = 0; j < JN; ++j)
+#pragma unroll
+        for (int i = 0; i < IN; ++i) {
+            const int y = warp + kWarps * j, x = lane + 32 * i;
+            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = cr[j][i];
+        }
+    __syncthreads();
+    // the last inverse step writes its outputs back where it read them (in place), so the
+    // numerators of placement row u sit in tile row u
+    fft::correlate_tile<N1, N2>(Z, RS, S, C, tw, neg, centre, tid, kThreads, BlockSync{},
+                                [&](int u, int v, float2 val) { Z[u * RS + v] = val; });
+    const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
+    float* out = part + ((long long)b * K + k) * C * C;
+    for (int idx = tid; idx < C * C; idx += kThreads) {
+        const int u = idx / C, v = idx - u * C;
+        out[idx] = Z[u * RS + v].x * scale;
+    }
+    if (tid == 0) {
+        scal[2 * ((long long)b * K + k)] = (double)centre.sx * a0;
+        scal[2 * ((long long)b * K + k) + 1] = sqrt(a1 * st);
+    }
+}
+
+// One CTA per pair: the sum of the K partial numerators of every placement (FP64, in block order,
+// plus the centring corrections), normalised by the chip's 1/|r'| and the placement's 1/sigma_box,
+// then the direct FP32 recomputation where the transform's bound is loose (spec_surface) and the
+// stage's outputs, as in spec_kernel.  g: the whole stage (R, W, C).  Shared memory: the
+// placement statistics and the surface (C^2 floats each) and a reduction scratch.
+__global__ void __launch_bounds__(kThreads, 1)
+spec_reduce_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
+                   int K, const ChipStat* cstat, InvSource inv, const float* part, const double* scal,
+                   SpecOut out)
+{
+    extern __shared__ __align__(16) unsigned char ssm[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    const int tid = threadIdx.x;
+    if (valid[p] < 0) {
+        if (out.stage == 0 && tid == 0) {
+            out.coarse[p] = CoarseOut{-1, -1, -1, -1};
+            out.coarse_peak[p] = NAN;
+        }
+        return;
+    }
+    const int R = g.R, W = g.W, C = g.C, CC = C * C;
+    float* invs = reinterpret_cast<float*>(ssm);
+    float* G = invs + ((CC + 3) & ~3);
+    double* red = reinterpret_cast<double*>(G + ((CC + 3) & ~3));
+    const float* inv_b = inv.off ? inv.base + inv.off[p] : inv.base + (long long)blockIdx.x * CC;
+    const long long is = inv.off ? inv.stride : C;
+    for (int idx = tid; idx < CC; idx += kThreads) {
+        const int u = idx / C, v = idx - u * C;
+        invs[idx] = __ldg(inv_b + u * is + v);
+    }
+    const double* sc = scal + 2 * (long long)blockIdx.x * K;
+    double corr = 0.0, errs = 0.0;
+    for (int k = 0; k < K; ++k) {
+        corr += sc[2 * k];
+        errs += sc[2 * k + 1];
+    }
+    const ChipStat cst = cstat[blockIdx.x];
+    const float inv_sigma = (float)cst.inv_sigma;
+    const float ebox = kSpecErr * (float)errs * inv_sigma;
+    __syncthreads();
+    float bv = -INFINITY;
+    int bi = INT_MAX;
+    int flagged = 0;
+    const float* pp = part + (long long)blockIdx.x * K * CC;
+    for (int idx = tid; idx < CC; idx += kThreads) {
+        double num = corr;
+        for (int k = 0; k < K; ++k) num += (double)__ldg(pp + (long long)k * CC + idx);
+        const float inv_box = invs[idx];
+        const float gv = (float)num * inv_box * inv_sigma;
+        G[idx] = gv;
+        if (ebox * inv_box > kSpecTol)
+            flagged = 1;
+        else
+            better(bv, bi, gv, idx);
+    }
+    __syncthreads();
+    const float* chip = spec_chip(src, pair0, blockIdx.x);
+    const float* win = spec_win(src, pair0, blockIdx.x);
+    float* surf = out.surfaces ? out.surfaces + (size_t)p * CC : nullptr;
+    float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * CC : nullptr;
+    spec_surface(G, red, g, invs, inv_sigma, cst.mean, ebox, chip, src.chip_stride, win, src.win_stride, gam,
+                 surf, bv, bi, flagged);
+    if (tid == 0) {
+        const int u = bi / C, v = bi - u * C;
+        if (out.stage == 0) {
+            // nudge.cu:107-140 (argument roles from nudge.cu:57: old = W, new = R + 2m)
+            const int E = R + 2 * out.m;
+            int left = v - out.m;
+            if (left < 0) left = 0;
+            if (left + E > W) left = W - E;
+            int top = u - out.m;
+            if (top < 0) top = 0;
+            if (top + E > W) top = W - E;
+            out.coarse[p] = CoarseOut{u, v, top, left};
+            out.coarse_peak[p] = bv;
+        } else {
+            out.fine[p] = FineOut{u, v, bv, 0.0f};
+        }
+    }
+}
+
+// The linear-phase steps of an n x n complex tile in global memory (rows `stride` apart), as
+// deramp_tile measures them: the phases of the lag-one autocorrelations along samples and lines.
+// red: 4 kWarps doubles; every thread gets both phases; ends with a barrier.
+__device__ void deramp_phases_global(const float2* t, long long stride, int n, double* red, float& ps, float& pl)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float sr = 0.0f, si = 0.0f, lr = 0.0f, li = 0.0f;
+    for (int k = tid; k < n * n; k += kThreads) {
+        const int y = k / n, x = k - y * n;
+        const float2 z = __ldg(t + y * stride + x);
+        if (x + 1 < n) {
+            const float2 w = __ldg(t + y * stride + x + 1);
+            sr = fmaf(w.x, z.x, fmaf(w.y, z.y, sr));
+            si = fmaf(w.y, z.x, fmaf(-w.x, z.y, si));
+        }
+        if (y + 1 < n) {
+            const float2 w = __ldg(t + (y + 1) * stride + x);
+            lr = fmaf(w.x, z.x, fmaf(w.y, z.y, lr));
+            li = fmaf(w.y, z.x, fmaf(-w.x, z.y, li));
+        }
+    }
+    double v[4] = {sr, si, lr, li};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) red[4 * warp + q] = v[q];
+    __syncthreads();
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < kWarps; ++w)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[q] += red[4 * w + q];
+    ps = (float)atan2(a[1], a[0]);
+    pl = (float)atan2(a[3], a[2]);
+    __syncthreads();
+}
+
+// Band-limited upsampling of tiles too large to stage whole (N up to 160, F = 2 N): the same
+// transforms as fft_upsample, the rows first, a strip of ST rows at a time (N-point FFTs, F-point
+// padded inverses) into a per-pair buffer in global memory (N x F complex, row-major), then the
+// columns of that buffer CB at a time (N-point FFTs, F-point padded inverses, amplitudes out).
+template <int N1, int N2, int F1, int F2>
+struct BigUpsampleGeom {
+    static constexpr int N = N1 * N2, F = F1 * F2, ST = 32, CB = 32;
+    static constexpr int XS = ST * (N + 1) > N * (CB + 1) ? ST * (N + 1) : N * (CB + 1);  // float2
+    static constexpr int YS = ST * (F + 1) > F * (CB + 1) ? ST * (F + 1) : F * (CB + 1);
+    static constexpr int smem = (XS + YS + N + F) * 8 + 4 * kWarps * 8;
+};
+
+template <int N1, int N2, int F1, int F2, bool DERAMP>
+__global__ void __launch_bounds__(kThreads, BigUpsampleGeom<N1, N2, F1, F2>::smem <= 113 * 1024 ? 2 : 1)
+spec_refine_big_kernel(const float2* base, const long long* off, long long stride, const CoarseOut* coarse,
+                       long long pair0, long long pairs, const long long* valid, const float2* twn_g,
+                       const float2* twf_g, float2* ybuf, float* refined, long long refined_stride,
+                       long long out_off)
+{
+    using G = BigUpsampleGeom<N1, N2, F1, F2>;
+    constexpr int N = G::N, F = G::F, ST = G::ST, CB = G::CB;
+    constexpr int RSN = N + 1, RSF = F + 1, CBS = CB + 1;
+    extern __shared__ __align__(16) unsigned char rsm[];
+    if (blockIdx.x >= pairs) return;
+    const long long p = pair0 + blockIdx.x;
+    if (valid[p] < 0) return;
+    const float2* src = base + off[p];
+    if (coarse) {
+        const CoarseOut co = coarse[p];
+        src += co.top * stride + co.left;
+    }
+    float2* X = reinterpret_cast<float2*>(rsm);
+    float2* Y = X + G::XS;
+    float2* twn = Y + G::YS;
+    float2* twf = twn + N;
+    double* red = reinterpret_cast<double*>(twf + F);
+    float2* yg = ybuf + (long long)blockIdx.x * N * F;
+    float* out = refined + (long long)blockIdx.x * refined_stride + out_off;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < N; q += kThreads) twn[q] = __ldg(twn_g + q);
+    for (int q = tid; q < F; q += kThreads) twf[q] = __ldg(twf_g + q);
+    float ps = 0.0f, pl = 0.0f;
+    if (DERAMP) deramp_phases_global(src, stride, N, red, ps, pl);
+    __syncthreads();
+    // rows, a strip at a time, into the buffer
+    for (int r0 = 0; r0 < N; r0 += ST) {
+        const int nr = N - r0 < ST ? N - r0 : ST;
+        for (int t = tid; t < nr * N; t += kThreads) {
+            const int y = t / N, x = t - y * N;
+            float2 z = __ldg(src + (long long)(r0 + y) * stride + x);
+            if (DERAMP) {
+                float s, c;
+                sincosf(fmaf(ps, (float)x, pl * (float)(r0 + y)), &s, &c);
+                z = make_float2(fmaf(z.x, c, z.y * s), fmaf(z.y, c, -z.x * s));
+            }
+            X[y * RSN + x] = z;
+        }
+        __syncthreads();
+        for (int t = tid; t < nr * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % nr) * RSN, 1, t / nr, twn);
+        __syncthreads();
+        for (int t = tid; t < nr * N1; t += kThreads) fft::step_b<N1, N2, -1>(X + (t % nr) * RSN, 1, t / nr);
+        __syncthreads();
+        for (int t = tid; t < nr * F1; t += kThreads)
+            fft::step_b_pad<N1, N2, F1, F2>(X + (t % nr) * RSN, 1, Y + (t % nr) * RSF, 1, t / nr);
+        __syncthreads();
+        for (int t = tid; t < nr * F2; t += kThreads) fft::inv_a<F1, F2>(Y + (t % nr) * RSF, 1, t / nr, twf);
+        __syncthreads();
+        for (int t = tid; t < nr * F; t += kThreads) {
+            const int y = t / F, x = t - y * F;
+            yg[(long long)(r0 + y) * F + x] = Y[y * RSF + x];
+        }
+        __syncthreads();
+    }
+    // columns of the buffer, CB at a time
+    const float scale = 1.0f / ((float)N * (float)N);
+    for (int c0 = 0; c0 < F; c0 += CB) {
+        const int nc = F - c0 < CB ? F - c0 : CB;
+        for (int t = tid; t < N * CB; t += kThreads) {
+            const int y = t / CB, cc = t - y * CB;
+            if (cc < nc) X[y * CBS + cc] = yg[(long long)y * F + c0 + cc];
+        }
+        __syncthreads();
+        for (int t = tid; t < CB * N2; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) fft::fwd_a<N1, N2>(X + cc, CBS, t / CB, twn);
+        }
+        __syncthreads();
+        for (int t = tid; t < CB * N1; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) fft::step_b<N1, N2, -1>(X + cc, CBS, t / CB);
+        }
+        __syncthreads();
+        for (int t = tid; t < CB * F1; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) fft::step_b_pad<N1, N2, F1, F2>(X + cc, CBS, Y + cc, CBS, t / CB);
+        }
+        __syncthreads();
+        for (int t = tid; t < CB * F2; t += kThreads) {
+            const int cc = t % CB;
+            if (cc < nc) {
+                float* col = out + c0 + cc;
+                fft::inv_a_store<F1, F2>(Y + cc, CBS, t / CB, twf, [&](int n, float2 v) {
+                    const float re = v.x * scale, im = v.y * scale;
+                    col[(long long)n * F] = sqrtf(re * re + im * im);
+                });
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// refinement lengths too large for fft_upsample: N, N1, N2, F1, F2 (F = 2 N)
+#define AMPCOR_REFINE_BIG(X) \
+    X(96, 8, 12, 12, 16)     \
+    X(120, 8, 15, 15, 16)    \
+    X(128, 8, 16, 16, 16)    \
+    X(144, 12, 12, 12, 24)   \
+    X(160, 10, 16, 16, 20)
+
 }  // namespace
 
 __global__ void detect_kernel(const float2* __restrict__ src, long long n, float* __restrict__ dst)
@@ -790,12 +1211,42 @@ bool spec_refine_supported(int n, int f, int& smem)
     return false;
 }
 
+bool spec_refine_big_supported(int n, int f, int& smem)
+{
+    if (f != 2) return false;
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)              \
+    if (n == NN) {                                      \
+        smem = BigUpsampleGeom<A, B, C, D>::smem;       \
+        return smem <= 227 * 1024;                      \
+    }
+    AMPCOR_REFINE_BIG(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    return false;
+}
+
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
-                               long long refined_stride, long long out_off, int deramp)
+                               long long refined_stride, long long out_off, int deramp,
+                               float2* ybuf)
 {
+    int small_smem = 0;
+    if (!spec_refine_supported(n, 2, small_smem) && ybuf) {
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                              \
+        if (n == NN) {                                                                                  \
+            if (deramp)                                                                                 \
+                spec_refine_big_kernel<A, B, C, D, true><<<blocks, kThreads, BigUpsampleGeom<A, B, C, D>::smem, st>>>( \
+                    base, off, stride, coarse, pair0, pairs, valid, twn, twf, ybuf, refined, refined_stride, out_off); \
+            else                                                                                        \
+                spec_refine_big_kernel<A, B, C, D, false><<<blocks, kThreads, BigUpsampleGeom<A, B, C, D>::smem, st>>>( \
+                    base, off, stride, coarse, pair0, pairs, valid, twn, twf, ybuf, refined, refined_stride, out_off); \
+            return cudaGetLastError();                                                                  \
+        }
+        AMPCOR_REFINE_BIG(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+        return cudaErrorInvalidValue;
+    }
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                           \
     if (n == NN) {                                                                                   \
         if (deramp)                                                                                  \
@@ -824,11 +1275,86 @@ cudaError_t spec_set_smem_limits()
 #undef AMPCOR_REFINE_CASE
 #define AMPCOR_SPEC_CASE(NN, A, B) \
     if (e == cudaSuccess)          \
-        e = cudaFuncSetAttribute(spec_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+        e = cudaFuncSetAttribute(spec_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess)          \
+        e = cudaFuncSetAttribute(spec_block_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
 #undef AMPCOR_SPEC_CASE
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D) \
+    if (e == cudaSuccess)                  \
+        e = cudaFuncSetAttribute(spec_refine_big_kernel<A, B, C, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess)                  \
+        e = cudaFuncSetAttribute(spec_refine_big_kernel<A, B, C, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    AMPCOR_REFINE_BIG(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spec_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spec_tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     return e;
 }
+
+cudaError_t launch_spec_chip_stats(unsigned blocks, cudaStream_t st, SpecSource src, long long pair0,
+                                   long long pairs, const long long* valid, int R, ChipStat* out)
+{
+    spec_chip_stats_kernel<<<blocks, 256, 0, st>>>(src, pair0, pairs, valid, R, out);
+    return cudaGetLastError();
+}
+
+// placement rows per pass of the tile statistics (two CTAs per SM where the window allows) and
+// the shared memory that takes; 0 when the window is wider than a CTA has threads
+int spec_tile_stats_rows(int W, int C, int& smem)
+{
+    smem = 0;
+    if (W > kThreads || C < 1) return 0;
+    // window_stats_xs hands each placement row of a pass to one warp
+    int sr = C < kWarps ? C : kWarps;
+    while (sr > 1 && 2L * sr * (W + 1) * 8 > 110L * 1024) --sr;
+    smem = (int)(2L * sr * (W + 1) * 8);
+    return smem <= 227 * 1024 ? sr : 0;
+}
+
+cudaError_t launch_spec_tile_stats(unsigned blocks, cudaStream_t st, SpecSource src, long long pair0,
+                                   long long pairs, const long long* valid, int R, int W, float* inv)
+{
+    int smem = 0;
+    const int sr = spec_tile_stats_rows(W, W - R + 1, smem);
+    if (!sr) return cudaErrorInvalidValue;
+    spec_tile_stats_kernel<<<blocks, kThreads, smem, st>>>(src, pair0, pairs, valid, R, W, sr, inv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spec_block(const SpecGeom& tile, int nb, unsigned blocks, cudaStream_t st,
+                              SpecSource src, long long pair0, long long pairs,
+                              const long long* valid, const ChipStat* cstat, const float2* tw,
+                              float* part, double* scal)
+{
+#define AMPCOR_SPEC_CASE(NN, A, B)                                                                   \
+    if (tile.N == NN) {                                                                              \
+        spec_block_kernel<A, B><<<blocks, kThreads, tile.smem_bytes, st>>>(src, pair0, pairs, valid, \
+                                                                           tile, nb, cstat, tw, part, scal); \
+        return cudaGetLastError();                                                                   \
+    }
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return cudaErrorInvalidValue;
+}
+
+int spec_reduce_smem(int C)
+{
+    return 2 * ((C * C + 3) & ~3) * 4 + 256;
+}
+
+cudaError_t launch_spec_reduce(const SpecGeom& full, int K, unsigned blocks, cudaStream_t st,
+                               SpecSource src, long long pair0, long long pairs,
+                               const long long* valid, const ChipStat* cstat, InvSource inv,
+                               const float* part, const double* scal, SpecOut out)
+{
+    spec_reduce_kernel<<<blocks, kThreads, spec_reduce_smem(full.C), st>>>(src, pair0, pairs, valid, full, K,
+                                                                           cstat, inv, part, scal, out);
+    return cudaGetLastError();
+}
+
 
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
                         long long pair0, long long pairs, const long long* valid, InvSource inv,

@@ -224,10 +224,37 @@ def production_4096(n=120, heavy_tail=False):
     return Workload(name, ref, tgt, ulhc, kept, 64, 32, 2, 8, 8, truth)
 
 
+def grid_4096(chip, margin, n, spacing, heavy_tail=False, refine_margin=8, zoom=8):
+    """production_4096's rasters with another tile geometry: an n x n grid of chip x chip tiles
+    spaced ``spacing`` px apart, centred on the raster, +-margin px search, refine 2 / margin
+    ``refine_margin``, zoom ``zoom``.  Pairs whose window would leave the raster are dropped as
+    Plan.assemble drops them."""
+    base = production_4096(heavy_tail=heavy_tail)
+    shape = base.ref.shape
+    cy, cx = quadratic_field(3, 10.0)
+    span = spacing * (n - 1)
+    first = (shape[0] - span) // 2
+    ticks = [first + spacing * k for k in range(n)]
+    centres = [(a, b) for a in ticks for b in ticks]
+    ulhc, kept = _grid_pairs(shape, centres, chip, margin)
+    truth = np.stack([field_at(cy, shape, kept[:, 0], kept[:, 1]),
+                      field_at(cx, shape, kept[:, 0], kept[:, 1])], axis=1)
+    name = f"chip{chip}_margin{margin}_4096"
+    return Workload(name, base.ref, base.tgt, ulhc, kept, chip, margin, 2, refine_margin, zoom, truth)
+
+
+def reference_default_4096():
+    """The reference's default correlation geometry (pkg/ampcor/correlators/MGA.py:28-42:
+    128 x 128 chips, 32 px padding, refine factor 2 with an 8 px margin, zoom 8) on
+    production_4096's rasters: a 60 x 60 grid of chips 64 px apart, 3,600 pairs."""
+    return grid_4096(128, 32, 60, 64)
+
+
 WORKLOADS = {
     "plain_512": plain_512,
     "production_4096": production_4096,
     "heavy_tail_4096": lambda: production_4096(heavy_tail=True),
+    "reference_default_4096": reference_default_4096,
 }
 
 

@@ -196,6 +196,19 @@ def fp32_peak(device):
     return lib.fp32_fma_tflops(device, 5)
 
 
+SPEC_LENGTHS = (16, 24, 32, 40, 48, 64, 80, 96, 120, 128, 144, 160)
+
+
+def spec_length(w):
+    """The transform length the spectral form uses for a window of w samples."""
+    return next((n for n in SPEC_LENGTHS if n >= w), 0)
+
+
+def fft_flops(n):
+    """Arithmetic of one complex n-point FFT, by the usual 5 n log2 n count."""
+    return 5.0 * n * np.log2(n) if n > 1 else 0.0
+
+
 def load_traffic():
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
@@ -413,6 +426,24 @@ def run_b200(args):
                           "unit": unit, "frac": achieved / peak, "ms_per_step": k_ms / args.steps,
                           "amount_per_region": amount, "ms_per_region": region_ms,
                           "traffic": tr["bytes_per_pair"] * pairs_per_region if tr else None}
+        if worker.form == "spectral":
+            # the spectral kernels are bound by instruction issue, not by memory: their FFT
+            # arithmetic (5 N log2 N flops per complex N-point transform) against the measured FP32
+            # FMA peak
+            nc, nf = spec_length(W), spec_length(Wf)
+            fft = {
+                "coarse_correlation": (W + 2 * nc + C) * fft_flops(nc),
+                "fine_correlation": (Wf + 2 * nf + Cf) * fft_flops(nf),
+                "refinement": sum(n * fft_flops(n) + n * fft_flops(f * n) + f * n * fft_flops(n)
+                                  + f * n * fft_flops(f * n) for n in (R, E)),
+            }
+            for k, per_pair in fft.items():
+                if k in kernels:
+                    kk = kernels[k]
+                    t = per_pair * (kk["amount_per_region"] / work[k][1]) / (kk["ms_per_region"] / 1e3) / 1e12
+                    kk["fft_flops_per_pair"] = per_pair
+                    kk["fft_tflops"] = t
+                    kk["fft_frac_of_fp32_simt"] = t / simt
         top = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
         topk = kernels[top]
         cpu = None
@@ -441,6 +472,7 @@ def run_b200(args):
                               f"(one chunk of pairs) / its CUDA-event time; traffic from "
                               f"profiles/traffic.json (ncu)"),
                 "fp32_simt_peak": simt,
+                "top_kernel_fft_frac_of_fp32_simt": topk.get("fft_frac_of_fp32_simt"),
                 "kernels": kernels,
                 "kernel_ms_per_step": {names[k]: v[0] / args.steps for k, v in kt.items() if v[1]},
                 "launches_per_step": {names[k]: v[1] / args.steps for k, v in kt.items() if v[1]},
