@@ -105,6 +105,7 @@ SIGNATURES = {
     "ampcor_form": (c_int, [c_void_p]),
     "ampcor_configure": (c_int, [c_void_p, c_int, c_uint64]),
     "ampcor_chunk": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "ampcor_inject_timeout": (c_int, [c_void_p, c_int]),
     "ampcor_correlate_noalloc": (c_int, [POINTER(Params), POINTER(Job), c_void_p, ctypes.c_char_p,
                                          ctypes.c_size_t]),
     "ampcor_last_error": (c_char_p, [c_void_p]),

@@ -355,7 +355,7 @@ bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
     g.off_glo = (int)(off += plane_g);
     off += plane_g;
     g.off_bar = (int)off;
-    off += 32;  // four mbarriers
+    off += 48;  // five mbarriers (the fifth is waited on only by failure-detection tests)
     g.off_misc = (int)off;
     off += 128;
     g.smem_bytes = (int)off;
@@ -531,6 +531,8 @@ struct ampcor_handle {
     FineOut* d_fine_out = nullptr;
     size_t fine_cap = 0;
     unsigned int* d_tc_err = nullptr;
+    // batches whose tensor-core zoom is made to time out (ampcor_inject_timeout)
+    int inject_timeouts = 0;
     // per-kernel timing: (start, stop) event pairs of each launch, per kernel kind
     // (0 coarse correlation, 1 refinement, 2 fine correlation, 3 coarse statistics,
     //  4 fine statistics, 5 zoom)
@@ -767,7 +769,7 @@ int launch_zoom(ampcor_handle* h, long long c0, unsigned n, const PairSource& sr
         const unsigned blocks = std::min<unsigned>(n, 148u);
         tc_zoom_kernel<<<blocks, 256, h->ztc.smem_bytes, st>>>(
             h->d_gam, c0, n, src.ref_off, h->ztc, h->d_zoom_uhl, h->d_coarse, h->d_coarse_peak,
-            h->d_fine_out, h->M, h->f, h->m, compat, offsets, diag, h->d_tc_err);
+            h->d_fine_out, h->M, h->f, h->m, compat, offsets, diag, h->d_tc_err, h->inject_timeouts > 0 ? 1 : 0);
     } else {
         zoom_kernel<<<n, 256, h->zoom_smem, st>>>(h->d_gam, c0, n, src.ref_off, h->zg, h->d_zoom_ut,
                                                   h->d_coarse, h->d_coarse_peak, h->d_fine_out, h->M,
@@ -997,14 +999,19 @@ int run_spectral(ampcor_handle* h, const PairSource& src, long long pairs, float
 int run_pipeline(ampcor_handle* h, const PairSource& src, long long pairs, float2* offsets,
                  PairDiag* diag, float* coarse_surfaces, float* refined_surfaces, cudaStream_t st)
 {
+    int rc;
     switch (h->form) {
         case kFormSpectral:
-            return run_spectral(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+            rc = run_spectral(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+            break;
         case kFormTensor:
-            return run_tensor(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+            rc = run_tensor(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+            break;
         default:
-            return run_plain(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
+            rc = run_plain(h, src, pairs, offsets, diag, coarse_surfaces, refined_surfaces, st);
     }
+    if (h->inject_timeouts > 0) --h->inject_timeouts;
+    return rc;
 }
 
 cudaStream_t pick(ampcor_handle* h, void* stream)
@@ -1598,6 +1605,16 @@ int ampcor_configure(ampcor_handle* h, int form, uint64_t chunk)
         // a form switch needs the chunk scratch of the new form
         free_chunk_scratch(h);
     }
+    return AMPCOR_OK;
+}
+
+int ampcor_inject_timeout(ampcor_handle* h, int batches)
+{
+    if (!h) return AMPCOR_E_ARG;
+    if (batches < 0) return fail(h, AMPCOR_E_ARG, "batches must not be negative");
+    if (!h->zoom_tc || h->form == kFormPlain)
+        return fail(h, AMPCOR_E_STATE, "the worker's form has no bounded tensor-core waits");
+    h->inject_timeouts = batches;
     return AMPCOR_OK;
 }
 

@@ -194,13 +194,15 @@ struct ZoomTcGeom {
 };
 
 // zoom of the refined surfaces of a chunk on the tensor cores; same outputs as zoom_kernel.
-// uhl: the hi and lo planes of U, contiguous.  One CTA per SM walks the pairs.
+// uhl: the hi and lo planes of U, contiguous.  One CTA per SM walks the pairs.  stall != 0 (a
+// failure-detection test) makes every CTA's first wait on a barrier nothing completes: the
+// bounded wait runs out before any work is issued and the chunk reports a time-out in err_out.
 __global__ void tc_zoom_kernel(const float* gam, long long pair0, long long pairs,
                                const long long* ref_off, ZoomTcGeom zt, const float* uhl,
                                const CoarseOut* coarse, const float* coarse_peak,
                                const FineOut* fout, int margin, int refine_factor,
                                int refine_margin, int ref_compat, float2* offsets, PairDiag* diag,
-                               unsigned int* err_out);
+                               unsigned int* err_out, int stall);
 
 // spectral form: FFT correlation of one tile pair per CTA (512 threads, one CTA per SM).  The
 // N x N tile (N = N1 N2 >= W, row stride RS = N + 1 complex samples) holds the window in its real

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kZThreads, 1)
 tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long long* ref_off,
                ZoomTcGeom zt, const float* uhl, const CoarseOut* coarse, const float* coarse_peak,
                const FineOut* fout, int margin, int refine_factor, int refine_margin, int ref_compat,
-               float2* offsets, PairDiag* diag, unsigned int* err_out)
+               float2* offsets, PairDiag* diag, unsigned int* err_out, int stall)
 {
     extern __shared__ __align__(1024) unsigned char zsm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -62,6 +62,7 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
     uint64_t* bar = reinterpret_cast<uint64_t*>(zsm + zt.off_bar);  // the first product
     uint64_t* drain = bar + 1;
     uint64_t* ubar = bar + 2;  // the two accumulator buffers of Zm
+    uint64_t* never = bar + 4;  // completed by nothing: the wait of a failure-detection test
     unsigned char* misc = zsm + zt.off_misc;
     uint32_t* tmem_s = reinterpret_cast<uint32_t*>(misc);
     volatile int* err = reinterpret_cast<volatile int*>(misc + 8);
@@ -79,6 +80,7 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         mbar_init(drain, 1);
         mbar_init(ubar, 1);
         mbar_init(ubar + 1, 1);
+        mbar_init(never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -117,7 +119,15 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         return ok;
     };
 
-    for (long long b = blockIdx.x; b < pairs; b += gridDim.x) {
+    // a failure-detection test: before any tensor-core work is issued, every thread waits on a
+    // barrier that nothing completes; the bounded wait runs out, sets the error flag, and the CTA
+    // skips its pairs and reports the time-out like any other expired wait
+    if (stall) {
+        mbar_wait(never, 0u, err, kStallCycles);
+        __syncthreads();
+    }
+
+    for (long long b = blockIdx.x; b < pairs && !*err; b += gridDim.x) {
         const long long p = pair0 + b;
         if (ref_off[p] < 0) {
             if (tid == 0) {

@@ -38,19 +38,24 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
     return done != 0;
 }
 
-// wait for the phase of the given parity; false once the error flag is set or the bound expires
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err)
+// wait for the phase of the given parity; false once the error flag is set or the bound (cycles)
+// expires, which sets the flag
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err,
+                                          long long bound = kSpinCycles)
 {
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
         if (*err) return false;
-        if (clock64() - t0 > kSpinCycles) {
+        if (clock64() - t0 > bound) {
             *err = 1;
             return false;
         }
     }
     return true;
 }
+
+// the bound of a wait made to run out by a failure-detection test (about a millisecond)
+constexpr long long kStallCycles = 1ll << 21;
 
 __device__ __forceinline__ void fence_async_smem()
 {

@@ -41,6 +41,7 @@ class Job:
     start: float | None = None
     done: float | None = None
     offsets: np.ndarray | None = None
+    error: str | None = None       # why the job was refused, if it was
 
     @property
     def pairs(self):
@@ -51,7 +52,33 @@ class Job:
         return (self.chip, self.margin, self.refine_factor, self.refine_margin, self.zoom_factor)
 
     def device_bytes(self):
-        return 2 * self.ref.numel() * 8 + self.pairs * (16 + 8)
+        """Device memory the job holds while it runs: both rasters (complex64), its corners and
+        its offsets.  The workers' own scratch (sized once per geometry and slot by
+        :meth:`Server.warm`) is outside the budget the server admits against."""
+        return (self.ref.numel() + self.tgt.numel()) * 8 + self.pairs * (16 + 8)
+
+
+class Admission:
+    """First-come admission of jobs by device memory.  A job is admitted when its bytes fit in
+    what the budget has left; the oldest waiting job blocks the ones behind it (no overtaking),
+    and a job larger than the whole budget is refused at once, since it could never run."""
+
+    def __init__(self, budget):
+        self.budget = int(budget)
+        self.in_use = 0
+
+    def never_fits(self, job):
+        return job.device_bytes() > self.budget
+
+    def try_admit(self, job):
+        need = job.device_bytes()
+        if self.in_use + need > self.budget:
+            return False
+        self.in_use += need
+        return True
+
+    def release(self, job):
+        self.in_use -= job.device_bytes()
 
 
 def synth_pair(lines, samples, shift, seed, device, snr_db=10.0):
@@ -119,7 +146,10 @@ def poisson_jobs(n_jobs, rate=20.0, seed=7, device="cuda:0", sizes=(1024, 2048, 
 
 
 class Server:
-    """Runs jobs with up to ``slots`` in flight on ``device``, admitting by free device memory."""
+    """Runs jobs with up to ``slots`` in flight on ``device``, admitting by free device memory.
+
+    The budget is ``memory_budget`` bytes, or else 80 % of the device memory that is free once
+    :meth:`warm` has created the workers (whose scratch is therefore not counted twice)."""
 
     def __init__(self, device=0, slots=4, memory_budget=None, plain=False):
         import torch
@@ -129,9 +159,18 @@ class Server:
         self.plain = plain
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.workers = [dict() for _ in range(slots)]
-        free, total = torch.cuda.mem_get_info(self.device)
-        self.budget = memory_budget if memory_budget is not None else int(free * 0.8)
-        self.in_use = 0
+        self.fixed_budget = memory_budget
+        self.admission = Admission(memory_budget if memory_budget is not None else self._free_budget())
+
+    def _free_budget(self):
+        import torch
+
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return int(free * 0.8)
+
+    @property
+    def budget(self):
+        return self.admission.budget
 
     def _worker(self, slot, job):
         ws = self.workers[slot]
@@ -173,6 +212,9 @@ class Server:
                     u = torch.from_numpy(job.ulhc).to(self.device)
                     w.correlate(ref, tgt, u, stream=self.streams[slot])
         torch.cuda.synchronize(self.device)
+        if self.fixed_budget is None:
+            torch.cuda.empty_cache()
+            self.admission = Admission(self._free_budget())
 
     def _launch(self, slot, job, now):
         import torch
@@ -213,19 +255,20 @@ class Server:
                     job, ev, host, keep = r
                     job.done = time.perf_counter() - t0
                     job.offsets = host.numpy().copy()
-                    self.in_use -= job.device_bytes()
+                    self.admission.release(job)
                     running[s] = None
                     finished += 1
+            while pending and self.admission.never_fits(pending[0]):
+                job = pending.popleft()
+                job.error = (f"needs {job.device_bytes()} bytes of device memory, more than the "
+                             f"server's budget of {self.admission.budget}")
+                job.done = now
+                finished += 1
             for s in range(self.slots):
                 if running[s] is None and pending:
-                    job = pending[0]
-                    if self.in_use + job.device_bytes() > self.budget and self.in_use > 0:
+                    if not self.admission.try_admit(pending[0]):
                         break
-                    pending.popleft()
-                    self.in_use += job.device_bytes()
-                    running[s] = self._launch(s, job, now)
-            if not realtime and not queue and not pending and all(r is not None for r in running if r):
-                pass
+                    running[s] = self._launch(s, pending.popleft(), now)
             time.sleep(0.0002)
         for s in range(self.slots):
             for w in self.workers[s].values():
@@ -234,13 +277,17 @@ class Server:
 
 
 def latency_report(jobs):
-    """p50 / p99 job latency (ms), pairs/s over the busy span, and offset error vs the shifts."""
+    """p50 / p99 job latency (ms), pairs/s over the busy span, and offset error vs the shifts,
+    over the jobs that ran (refused ones are counted apart)."""
+    refused = [j for j in jobs if j.error]
+    jobs = [j for j in jobs if not j.error]
     lat = np.array([(j.done - j.arrival) * 1e3 for j in jobs])
     pairs = sum(j.pairs for j in jobs)
     span = max(j.done for j in jobs) - min(j.arrival for j in jobs)
     errs = [np.abs(j.offsets - np.asarray(j.truth)[None, :]).max() for j in jobs if j.truth]
     return {
         "jobs": len(jobs),
+        "refused": len(refused),
         "pairs": pairs,
         "p50_ms": float(np.percentile(lat, 50)),
         "p99_ms": float(np.percentile(lat, 99)),

@@ -141,6 +141,12 @@ class Worker:
                self._lib.ampcor_configure(self._handle, f, int(chunk or 0)))
         self.form = FORMS[self._lib.ampcor_form(self._handle)]
 
+    def inject_timeout(self, batches=1):
+        """Failure-detection test hook: the next ``batches`` batches make their tensor-core zoom
+        wait on a barrier nothing completes; the bounded wait runs out and the batch raises
+        :class:`Error` (AMPCOR_E_CUDA, timed out) at its synchronisation."""
+        _check(self._lib, self._handle, self._lib.ampcor_inject_timeout(self._handle, int(batches)))
+
     @property
     def chunk(self):
         c = ctypes.c_uint64()

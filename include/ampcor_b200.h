@@ -202,6 +202,15 @@ int ampcor_form(const ampcor_handle* handle);
    the worker's stream.  No reference counterpart. */
 int ampcor_configure(ampcor_handle* handle, int form, uint64_t chunk);
 
+/* Failure-detection test hook (no reference counterpart; the reference has no bounded waits).
+   The next `batches` batches of the worker (tensor-core or spectral form) make the first wait of
+   their tensor-core zoom on a barrier that nothing completes, bounded at about a millisecond:
+   every wait of the tensor-core kernels is bounded in time, and an expired wait stops the kernel
+   cleanly and is reported.  The zoom issues no work after it and writes no offsets for those
+   batches, and the ampcor_synchronize() that ends each of them returns AMPCOR_E_CUDA with a
+   time-out message; the worker stays usable.  0 switches it off. */
+int ampcor_inject_timeout(ampcor_handle* handle, int batches);
+
 /* The number of pairs refined per chunk. */
 int ampcor_chunk(const ampcor_handle* handle, uint64_t* chunk);
 

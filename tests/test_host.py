@@ -69,3 +69,28 @@ def test_ext_module_surface():
                  "Error"):
         assert hasattr(ampcor_cuda, name)
     assert "ampcor_b200" in ampcor_cuda.version()
+
+
+class _FakeJob:
+    def __init__(self, nbytes):
+        self.nbytes = nbytes
+
+    def device_bytes(self):
+        return self.nbytes
+
+
+def test_serving_admission_by_device_memory():
+    # jobs are admitted while their bytes fit in what the budget has left, released on
+    # completion, and a job larger than the whole budget is refused (it could never run)
+    from ampcor_b200.serve import Admission
+
+    a = Admission(100)
+    j1, j2, j3, big = _FakeJob(60), _FakeJob(30), _FakeJob(20), _FakeJob(101)
+    assert a.try_admit(j1) and a.try_admit(j2)
+    assert not a.try_admit(j3) and a.in_use == 90
+    assert a.never_fits(big) and not a.never_fits(j3)
+    a.release(j1)
+    assert a.try_admit(j3) and a.in_use == 50
+    a.release(j2)
+    a.release(j3)
+    assert a.in_use == 0
