@@ -70,7 +70,7 @@ def _warp_device(ref, dy0, dx0, quad, seed):
 
 def uneven_jobs(n=16, seed=11, device="cuda:0", shapes=((1024, 1024), (2048, 2048), (4096, 2048),
                                                          (8192, 2048), (2048, 4096)),
-                chips=(32, 64), margins=(8, 16, 32), spacing=(16, 128), max_offset=16.0):
+                chips=(32, 64, 128), margins=(8, 16, 32, 64), spacing=(16, 128), max_offset=16.0):
     """``n`` seeded raster pairs with uneven shapes and geometries (see module docstring)."""
     import torch
 

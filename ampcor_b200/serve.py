@@ -116,11 +116,12 @@ def grid_corners(lines, samples, chip, margin, spacing):
 
 def poisson_jobs(n_jobs, rate=20.0, seed=7, device="cuda:0", sizes=(1024, 2048, 3072, 4096),
                  chips=(32, 64), margins=(16, 32), zooms=(8, 16), refine_factor=2,
-                 refine_margin=8, spacing=(64, 128), pinned=True):
-    """A seeded Poisson stream of jobs (mean ``rate`` jobs/s): raster sides drawn from ``sizes``,
-    chip / margin / zoom from their lists, grid spacing from ``spacing``, a random sub-pixel shift
-    of at most 8 px.  Rasters are generated on the device and copied to pinned host memory so that
-    each job's upload is part of its latency."""
+                 refine_margin=8, spacing=(64, 128), pinned=True, square=False):
+    """A seeded Poisson stream of jobs (mean ``rate`` jobs/s): raster sides drawn from ``sizes``
+    (one side for both axes with ``square``), chip / margin / zoom from their lists, grid spacing
+    from ``spacing``, a random sub-pixel shift of at most 8 px.  Rasters are generated on the
+    device and, with ``pinned``, copied to pinned host memory so that each job's upload is part of
+    its latency."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -129,7 +130,7 @@ def poisson_jobs(n_jobs, rate=20.0, seed=7, device="cuda:0", sizes=(1024, 2048, 
     for jid in range(n_jobs):
         t += rng.exponential(1.0 / rate)
         lines = int(rng.choice(sizes))
-        samples = int(rng.choice(sizes))
+        samples = lines if square else int(rng.choice(sizes))
         chip = int(rng.choice(chips))
         margin = int(rng.choice(margins))
         zoom = int(rng.choice(zooms))

@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--no-geometries", action="store_true",
+                    help="skip the chip-128 (reference default geometry) line")
     ap.add_argument("--serving-jobs", type=int, default=40)
     return ap.parse_args()
 
@@ -395,7 +397,8 @@ def run_b200(args):
             "refinement": {"spectral": "spec_refine_kernel (chip + window)"}.get(worker.form, "refine_kernel"),
             "coarse_statistics": {"spectral": "detect_kernel + box_vsum_kernel + box_inv_kernel (per raster)"}
             .get(worker.form, "window_stats_cplx_kernel"),
-            "fine_statistics": "window_stats_real_kernel",
+            "fine_statistics": {"spectral": "spec_chip_stats_kernel + spec_tile_stats_kernel (blocked fine stage)"}
+            .get(worker.form, "window_stats_real_kernel"),
             "zoom": "tc_zoom_kernel (zoom_kernel where Zm exceeds the tensor memory)",
         }
         peaks = {}
@@ -487,6 +490,8 @@ def run_b200(args):
             line["cpu_baseline"] = cpu
         if parity_rep:
             line["parity"] = parity_rep
+        if world == 1 and not args.no_geometries:
+            line["reference_default_geometry"] = geometry_run("reference_default_4096", local, args)
         if world == 1 and not args.no_serving:
             line["serving"] = serving_run(local, args)
         if world == 1 and not args.no_uneven:
@@ -548,20 +553,98 @@ def cpu_leg(w, worker, ref, tgt, ulhc, timed_offsets):
 
 
 def serving_run(device, args):
-    """p50 / p99 job latency of the continuous-batching loop under a seeded Poisson stream."""
+    """The continuous-batching loop over the serving range (square rasters of 1024^2 to 8192^2,
+    chips 32-128, margins 16-64, refine 2, zoom 8-16): p50 / p99 job latency under a seeded Poisson
+    stream of 20 jobs/s with each job's upload from pinned host memory inside its latency, then the
+    same jobs queued all at once with their rasters in device memory (the rate the loop sustains
+    when work waits)."""
+    import dataclasses
+
+    import torch
+
     from ampcor_b200 import serve
 
     jobs = serve.poisson_jobs(args.serving_jobs, rate=20.0, seed=7, device=f"cuda:{device}",
-                              sizes=(1024, 2048, 4096), chips=(32, 64), margins=(16, 32),
-                              zooms=(8, 16), spacing=(64, 128), pinned=False)
-    srv = serve.Server(device=device, slots=4)
+                              sizes=(1024, 2048, 4096, 8192), chips=(32, 64, 128),
+                              margins=(16, 32, 64), zooms=(8, 16), spacing=(64, 128), pinned=True,
+                              square=True)
+    srv = serve.Server(device=device, slots=3)
     srv.warm(jobs)
     srv.run(jobs, realtime=True)
     rep = serve.latency_report(jobs)
-    rep["stream"] = (f"{args.serving_jobs} jobs, Poisson 20 jobs/s (seed 7), rasters 1024-4096 "
-                     f"px per side resident in HBM, chip 32/64, margin 16/32, refine 2, zoom 8/16, "
-                     f"4 slots")
+    dev = torch.device("cuda", device)
+    queued = [dataclasses.replace(j, arrival=0.0, ref=j.ref.to(dev), tgt=j.tgt.to(dev), start=None,
+                                  done=None, offsets=None) for j in jobs]
+    torch.cuda.synchronize(dev)
+    srv.run(queued, realtime=False)
+    sat = serve.latency_report(queued)
+    rep["saturation_pairs_per_s"] = sat["pairs_per_s"]
+    rep["saturation_span_ms"] = 1e3 * max(j.done for j in queued)
+    rep["saturation_same_offsets"] = all(np.array_equal(a.offsets, b.offsets) for a, b in zip(jobs, queued))
+    rep["geometries"] = len({j.geometry for j in jobs})
+    rep["stream"] = (f"{args.serving_jobs} jobs, Poisson 20 jobs/s (seed 7), square rasters of 1024, "
+                     f"2048, 4096 or 8192 px (upload from pinned host memory inside each job's "
+                     f"latency), chip 32/64/128, margin 16/32/64, refine 2, zoom 8/16, 3 slots; "
+                     f"saturation: the same jobs queued at once, rasters in device memory")
     return rep
+
+
+def geometry_run(name, device, args):
+    """Throughput of another tile geometry beside the headline: workload ``name`` autotuned,
+    warm-up and timed jobs with everything device-resident (CUDA events), then end to end through
+    ampcor_correlate_host with pinned host rasters."""
+    import torch
+
+    from ampcor_b200 import synth
+    from ampcor_b200.autotune import tune
+    from ampcor_b200.worker import Worker
+
+    w = synth.workload(name)
+    dev = torch.device("cuda", device)
+    worker = Worker(pairs=w.pairs, chip=(w.chip, w.chip), window=(w.window, w.window),
+                    refine_factor=w.refine_factor, refine_margin=w.refine_margin,
+                    zoom_factor=w.zoom_factor, device=device)
+    ref = torch.from_numpy(w.ref).to(dev)
+    tgt = torch.from_numpy(w.tgt).to(dev)
+    ulhc = torch.from_numpy(w.ulhc).to(dev)
+    offsets = torch.empty((w.pairs, 2), dtype=torch.float32, device=dev)
+    tuned = tune(worker, ref, tgt, ulhc, forms=("spectral", "tensor", "plain"), use_cache=False)
+    for _ in range(max(args.warmup, 3)):
+        worker.correlate(ref, tgt, ulhc, offsets=offsets, synchronize=False)
+    steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    worker.profile(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        worker.correlate(ref, tgt, ulhc, offsets=offsets, synchronize=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    kt = worker.kernel_times()
+    worker.profile(False)
+    worker._lib.ampcor_synchronize(worker.handle, None)
+    ref_h = torch.empty(w.ref.shape, dtype=torch.complex64, pin_memory=True)
+    tgt_h = torch.empty(w.tgt.shape, dtype=torch.complex64, pin_memory=True)
+    ref_h.numpy()[...] = w.ref
+    tgt_h.numpy()[...] = w.tgt
+    un = np.ascontiguousarray(w.ulhc)
+    worker.correlate(ref_h.numpy(), tgt_h.numpy(), un)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        out = worker.correlate(ref_h.numpy(), tgt_h.numpy(), un)
+    e2e_s = (time.perf_counter() - t0) / 3
+    line = {
+        "workload": workload_config(w)["workload"], "pairs": w.pairs, "form": worker.form,
+        "chunk": worker.chunk, "steps": steps, "ms_per_job": ms, "pairs_per_s": w.pairs / (ms / 1e3),
+        "e2e_pairs_per_s": w.pairs / e2e_s,
+        "kernel_ms_per_job": {k: v[0] / steps for k, v in kt.items() if v[1]},
+        "tune": [(c["form"], c["chunk"], round(c["ms"], 3)) for c in tuned["candidates"]],
+        "results_finite": bool(np.isfinite(out).all()),
+    }
+    worker.close()
+    return line
 
 
 def uneven_run(device, args):
