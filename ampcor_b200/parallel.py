@@ -5,6 +5,7 @@ lib/libampcor_cuda/correlators/Sequential.icc:47-141), so a job splits into cont
 of tile centres, one band per rank, with no collective on the data path.  Each rank needs only
 the raster lines its band touches (:func:`band_lines`), so a rank can copy just that slab into its
 own HBM.  The only exchange is the final gather of the offset field (8 bytes per pair).
+:func:`correlate_sharded` puts the pieces together for one job.
 """
 from __future__ import annotations
 
@@ -52,3 +53,31 @@ def gather_offsets(local_offsets, local_index, total, group=None):
         keep = i >= 0
         full[i[keep].numpy()] = o[keep].numpy()
     return full
+
+
+def band(ref, tgt, ulhc, chip, window, rank, world):
+    """The slice of one job that ``rank`` correlates: its pair indices, the raster lines its
+    pairs read (reference and secondary, as views of the full rasters) and its corners rebased to
+    those lines."""
+    ulhc = np.asarray(ulhc).reshape(-1, 4)
+    idx = shard(ulhc, rank, world)
+    (r0, r1), (t0, t1) = band_lines(ulhc[idx], chip, window)
+    local = ulhc[idx].astype(np.int64) - np.array([r0, 0, t0, 0], np.int64)
+    return idx, ref[r0:r1], tgt[t0:t1], np.ascontiguousarray(local, np.int32)
+
+
+def correlate_sharded(correlate, ref, tgt, ulhc, chip, window, group=None):
+    """Correlate one job over the ranks of ``group``: each rank takes its row band of pairs,
+    hands ``correlate(ref_band, tgt_band, ulhc_band)`` only the raster lines that band reads (so a
+    worker's host path uploads just those), and the offsets are gathered into the full field in
+    pair order on every rank.  ``correlate`` is typically ``Worker.correlate`` with host rasters."""
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    idx, ref_b, tgt_b, local = band(ref, tgt, ulhc, chip, window, rank, world)
+    if len(idx):
+        off = np.asarray(correlate(np.ascontiguousarray(ref_b), np.ascontiguousarray(tgt_b), local),
+                         np.float32).reshape(-1, 2)
+    else:
+        off = np.zeros((0, 2), np.float32)
+    return gather_offsets(off, idx, len(np.asarray(ulhc).reshape(-1, 4)), group=group)

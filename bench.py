@@ -7,7 +7,13 @@ production_4096: 4096x4096 complex64 speckle pair, 14,400 pairs of 64x64 chips, 
 refine factor 2 with an 8 px refine margin, zoom 8) run through the CUDA pipeline with rasters,
 pair corners and outputs resident in HBM.  Under torchrun every rank correlates its own job of
 the same size on its own GPU (weak scaling, no collective on the data path); ``value`` is the
-pairs of all ranks divided by the slowest rank's device time.
+pairs of all ranks divided by the slowest rank's device time.  With ``--shard`` the ranks split
+one job into row bands instead, each holding only the raster lines its band reads (strong
+scaling; ``value`` is the job's pairs over the slowest rank's time).
+
+Beside the headline the line carries the reference's default tile geometry (128 x 128 chips,
+32 px padding) as ``reference_default_geometry``, the serving loop over its whole range
+(``serving``: latency with uploads, and a saturation run) and the uneven batch in one CUDA graph.
 
 ``e2e`` is the same metric through the host entry point of the C ABI
 (ampcor_correlate_host): each step uploads both rasters and the corners from pinned host
@@ -60,6 +66,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="with several ranks, split one job into row bands (strong scaling) "
+                         "instead of running the job on every rank (weak scaling)")
     ap.add_argument("--no-geometries", action="store_true",
                     help="skip the chip-128 (reference default geometry) line")
     ap.add_argument("--serving-jobs", type=int, default=40)
@@ -282,6 +291,19 @@ def run_b200(args):
     if args.pairs:
         w.ulhc = w.ulhc[: args.pairs]
         w.truth = None if w.truth is None else w.truth[: args.pairs]
+    # job pairs all ranks process per step: the job on every rank (weak scaling), or one job
+    # split into row bands, each rank holding only the raster lines its band reads (strong)
+    shard = args.shard and world > 1
+    job_pairs = w.pairs * (1 if shard else world)
+    if shard:
+        import dataclasses
+
+        from ampcor_b200 import parallel
+
+        idx, ref_b, tgt_b, local = parallel.band(w.ref, w.tgt, w.ulhc, w.chip, w.window, rank, world)
+        w = dataclasses.replace(w, ref=np.ascontiguousarray(ref_b), tgt=np.ascontiguousarray(tgt_b),
+                                ulhc=local, centres=w.centres[idx],
+                                truth=None if w.truth is None else w.truth[idx])
     worker = Worker(pairs=w.pairs, chip=(w.chip, w.chip), window=(w.window, w.window),
                     refine_factor=w.refine_factor, refine_margin=w.refine_margin,
                     zoom_factor=w.zoom_factor, device=local, plain=args.plain)
@@ -339,7 +361,7 @@ def run_b200(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = world * w.pairs * args.steps / (ms_max / 1000.0)
+    value = job_pairs * args.steps / (ms_max / 1000.0)
 
     # end to end through the host entry point, pinned host buffers
     e2e_value, e2e_steps = None, 0
@@ -361,7 +383,7 @@ def run_b200(args):
         te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_value = world * w.pairs * e2e_steps / float(te.item())
+        e2e_value = job_pairs * e2e_steps / float(te.item())
         ok = ok and bool(np.isfinite(out).all())
 
     line = None
@@ -458,7 +480,7 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if shard else "weak", "vs_baseline": None,
             "dtype": "bf16x3" if worker.form == "tensor" else "f32",
             "data": "synthetic",
             "config": dict(workload_config(w), form=worker.form, chunk=worker.chunk,

@@ -1,7 +1,9 @@
 """Row-band sharding across ranks and the final offset gather, with two gloo ranks on CPU.
 
 Each rank correlates its own band (here with the FP64 oracle standing in for the GPU, since this
-runs without one) and the gathered field must equal the single-rank result pair for pair.
+runs without one) and the gathered field must equal the single-rank result pair for pair.  Through
+parallel.correlate_sharded a rank sees only the raster lines its band reads, with its corners
+rebased to them.
 """
 import os
 import socket
@@ -40,6 +42,64 @@ def _rank_main(rank, world, port, out):
         dist.barrier()
     finally:
         dist.destroy_process_group()
+
+
+def _band_main(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        w = synth.production_4096()
+        sub = w.ulhc[::97]
+        seen = {}
+
+        def correlate(ref_b, tgt_b, ulhc_b):
+            seen["lines"] = (ref_b.shape[0], tgt_b.shape[0])
+            off, _ = oracle.adjust(ref_b, tgt_b, ulhc_b, 64, 128, 2, 8, 8, threads=2)
+            return off
+
+        full = parallel.correlate_sharded(correlate, w.ref, w.tgt, sub, 64, 128)
+        np.save(f"{out}.{rank}.npy", full)
+        np.save(f"{out}.lines{rank}.npy", np.array(seen["lines"]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_correlate_sharded_uploads_bands_and_matches_one_rank(tmp_path):
+    import oracle
+
+    out = str(tmp_path / "field")
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_band_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    w = synth.production_4096()
+    sub = w.ulhc[::97]
+    want, _ = oracle.adjust(w.ref, w.tgt, sub, 64, 128, 2, 8, 8)
+    for r in range(2):
+        assert np.array_equal(np.load(f"{out}.{r}.npy"), want)
+        ref_lines, tgt_lines = np.load(f"{out}.lines{r}.npy")
+        assert ref_lines < 4096 * 0.6 and tgt_lines < 4096 * 0.6  # a band, not the raster
+    # the rebased corners address the same pixels as the original ones
+    for r in range(2):
+        idx, ref_b, tgt_b, local = parallel.band(w.ref, w.tgt, sub, 64, 128, r, 2)
+        for k in (0, len(idx) - 1):
+            a, b, c, d = local[k]
+            A, B, Cc, D = sub[idx[k]]
+            assert np.array_equal(ref_b[a:a + 64, b:b + 64], w.ref[A:A + 64, B:B + 64])
+            assert np.array_equal(tgt_b[c:c + 128, d:d + 128], w.tgt[Cc:Cc + 128, D:D + 128])
 
 
 def test_shards_partition_the_pairs():
