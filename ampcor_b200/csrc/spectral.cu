@@ -84,12 +84,15 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
 // The transform's error on a numerator is a small multiple of eps |r'| |t'| (|.|: Euclidean norms
 // of the zero-mean chip and the centred window; below 1.4e-7 |r'| |t'| over the compiled lengths
 // in host runs against FP64 sums), so its error on gamma is bounded by kSpecErr |t'| / sigma_box.
-// Where a box is nearly flat that bound grows; a placement whose bound exceeds kSpecTol has its
-// numerator recomputed as a direct FP32 sum whenever its value matters (it could be the maximum,
-// or the surface is returned).  Speckle never comes near the bound (|t'| / sigma_box is about
-// W / R); zero-padded or masked windows do.
+// Where a box is nearly flat that bound grows; a placement whose bound exceeds kSpecTol (half the
+// 2e-5 surface tolerance the parity tests hold every form to) has its numerator recomputed as a
+// direct FP32 sum whenever its value matters (it could be the maximum, or the surface is
+// returned).  On speckle the bound is about kSpecErr W / R (|t'| / sigma_box is about W / R, the
+// chip blocks of a blocked stage add theirs), 5e-6 for a 32 px chip in a +-64 px search
+// (W / R = 5), while the errors measured there stay below 3e-7; zero-padded or masked windows
+// exceed it.
 constexpr float kSpecErr = 1e-6f;
-constexpr float kSpecTol = 4e-6f;
+constexpr float kSpecTol = 1e-5f;
 
 // Scratch of the placement statistics while the chip waits in registers: slot k is the imaginary
 // part of tile sample k, and past the tile's nz samples it continues in the tail buffer.
