@@ -235,6 +235,8 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     off = up(off + (long)g.N * 8, 16);
     g.off_neg = (int)off;
     off = up(off + (long)g.N * 4, 16);
+    g.off_half = (int)off;  // one position of every Hermitian pair of the spectrum
+    off = up(off + (long)(g.N / 2 + 1) * 4, 16);
     g.off_red = (int)off;
     off += 256;
     g.off_inv = (int)off;  // the placement statistics, prefetched with the tiles
@@ -281,6 +283,8 @@ bool plan_spec_tile(int B, int S, int C, SpecGeom& g)
     off = up(off + (long)g.N * 8, 16);
     g.off_neg = (int)off;
     off = up(off + (long)g.N * 4, 16);
+    g.off_half = (int)off;
+    off = up(off + (long)(g.N / 2 + 1) * 4, 16);
     g.off_red = (int)off;
     off += 256;
     g.smem_bytes = (int)off;

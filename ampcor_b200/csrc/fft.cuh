@@ -408,20 +408,46 @@ HD void row_tasks(int rows, int J, int tid, int nt, F f)
     }
 }
 
+// The correlation spectrum is Hermitian (the correlation is real), so the inverse transform needs
+// one position of every pair (p, neg_pos(p)).  The half taken is {p : p <= neg_pos(p)}: in the
+// permuted order it is the block of positions N2 k1 + k2 with k1 below N1 / 2 (give or take the
+// ends), nearly contiguous, so lanes walking it hit distinct banks.  half_positions writes its N/2 + 1
+// positions in increasing order (one thread; the device builds the list with a warp ballot).
+template <int N1, int N2>
+HD constexpr int half_count() { return N1 * N2 / 2 + 1; }
+
+template <int N1, int N2>
+HD bool in_half(int p) { return p <= neg_pos<N1, N2>(p); }
+
+template <int N1, int N2>
+HD void half_positions(int* out)
+{
+    int c = 0;
+    for (int p = 0; p < N1 * N2; ++p)
+        if (in_half<N1, N2>(p)) out[c++] = p;
+}
+
 // ---- the 2-D correlation of one tile pair -------------------------------------------------
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)
 // holding t + i r: the window t in the real parts, the chip r in the imaginary parts, zero
 // outside them, centred on the way in as `centre` says.  Rows at and past rows_in are all zero.
-// neg[p] = neg_pos(p) for p < N.
+// neg[p] = neg_pos(p) for p < N; half: the half_positions list.
 // The correlation goes to store(u, v, value) for u < rows_out and v < N: value.x is
 // 4 N^2 sum_ij r(i, j) t(u + i, v + j)
-// (circular indices, which never wrap for the placements of a window of at most N samples).  The
-// tasks of each phase are spread over the nt threads; sync() separates the phases
-// (__syncthreads on the device).
+// (circular indices, which never wrap for the placements of a window of at most N samples); the
+// stores of a row go to rows of the tile no later step reads, so store may write into the tile's
+// rows below rows_out.  The tasks of each phase are spread over the nt threads; sync() separates
+// the phases (__syncthreads on the device).
+//
+// The inverse runs on the Hermitian half: the columns of the half only (N/2 + 1 of N), after which
+// every placement row is Hermitian along its row; two such rows A, B go through one transform as
+// A + i B (real and imaginary parts of the result), packed into the free rows past rows_out where
+// the tile has them, else each row is completed from its partners and transformed alone.
 template <int N1, int N2, class Sync, class Store>
 HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
-                       const int* neg, const Centre& centre, int tid, int nt, Sync sync, Store store)
+                       const int* neg, const int* half, const Centre& centre, int tid, int nt,
+                       Sync sync, Store store)
 {
     constexpr int N = N1 * N2;
     // forward along rows (centring the tile on the way in): lanes take consecutive rows
@@ -454,25 +480,59 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
         }
     }
     sync();
-    // inverse along columns
-    for (int t = tid; t < N * N1; t += nt) {
-        const int x = t % N, k1 = t / N;
-        step_b<N1, N2, 1>(Z + x, RS, k1);
+    // inverse along the columns of the Hermitian half
+    constexpr int NH = half_count<N1, N2>();
+    for (int t = tid; t < NH * N1; t += nt) {
+        const int c = t % NH, k1 = t / NH;
+        step_b<N1, N2, 1>(Z + half[c], RS, k1);
     }
     sync();
-    for (int t = tid; t < N * N2; t += nt) {
-        const int x = t % N, n2 = t / N;
-        inv_a<N1, N2>(Z + x, RS, n2, tw);
+    for (int t = tid; t < NH * N2; t += nt) {
+        const int c = t % NH, n2 = t / NH;
+        inv_a<N1, N2>(Z + half[c], RS, n2, tw);
     }
     sync();
-    // inverse along the rows that hold placements
-    row_tasks(rows_out, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, 1>(Z + y * RS, 1, k1); });
-    sync();
-    // the last step hands its outputs to store(u, v, value) instead of writing them back
-    row_tasks(rows_out, N2, tid, nt, [&](int y, int n2) {
-        inv_a_store<N1, N2>(Z + y * RS, 1, n2, tw, [&](int n, float2 v) { store(y, n, v); });
-    });
-    sync();
+    const int np = (rows_out + 1) / 2;
+    if (rows_out + np <= N) {
+        // placement rows 2q and 2q + 1 as one row A + i B at tile row rows_out + q; positions off
+        // the half take the conjugates of their partners
+        for (int t = tid; t < np * N; t += nt) {
+            const int q = t / N, x = t - q * N;
+            const int sx = in_half<N1, N2>(x) ? x : neg[x];
+            const float cj = sx == x ? 1.0f : -1.0f;
+            const float2 a = Z[2 * q * RS + sx];
+            const float2 b = 2 * q + 1 < rows_out ? Z[(2 * q + 1) * RS + sx] : make_float2(0.0f, 0.0f);
+            Z[(rows_out + q) * RS + x] = make_float2(a.x - cj * b.y, cj * a.y + b.x);
+        }
+        sync();
+        float2* P = Z + rows_out * RS;
+        row_tasks(np, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, 1>(P + y * RS, 1, k1); });
+        sync();
+        // the last step hands its outputs to store(u, v, value) instead of writing them back
+        row_tasks(np, N2, tid, nt, [&](int y, int n2) {
+            inv_a_store<N1, N2>(P + y * RS, 1, n2, tw, [&](int n, float2 v) {
+                store(2 * y, n, make_float2(v.x, 0.0f));
+                if (2 * y + 1 < rows_out) store(2 * y + 1, n, make_float2(v.y, 0.0f));
+            });
+        });
+        sync();
+    } else {
+        // every placement row completed from its partners, then transformed alone
+        for (int t = tid; t < rows_out * N; t += nt) {
+            const int y = t / N, x = t - y * N;
+            if (!in_half<N1, N2>(x)) {
+                const float2 v = Z[y * RS + neg[x]];
+                Z[y * RS + x] = make_float2(v.x, -v.y);
+            }
+        }
+        sync();
+        row_tasks(rows_out, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, 1>(Z + y * RS, 1, k1); });
+        sync();
+        row_tasks(rows_out, N2, tid, nt, [&](int y, int n2) {
+            inv_a_store<N1, N2>(Z + y * RS, 1, n2, tw, [&](int n, float2 v) { store(y, n, v); });
+        });
+        sync();
+    }
 }
 
 }  // namespace fft

@@ -211,7 +211,7 @@ struct SpecGeom {
     int R, W, C;      // chip, window, placements per axis
     int N, N1, N2;    // transform length and its two register radices
     int RS;           // tile row stride (complex samples)
-    int off_z, off_tw, off_neg, off_red, off_inv, off_gam;  // shared-memory byte offsets
+    int off_z, off_tw, off_neg, off_half, off_red, off_inv, off_gam;  // shared-memory byte offsets
     // placement statistics computed in the kernel (no InvSource given): nseg threads per window
     // column, their FP64 partial sums (4 nseg W doubles) at off_gam (the surface buffer, idle
     // until the last transform step), the column sums in the tile's imaginary parts and, past the

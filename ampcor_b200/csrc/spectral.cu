@@ -71,6 +71,23 @@ __device__ void block_sum2(double& a, double& b, double* red)
     __syncthreads();
 }
 
+// one warp: the positions of fft::half_positions (one member of every Hermitian pair of the
+// permuted spectrum, increasing), 32 candidates per ballot
+template <int N1, int N2>
+__device__ void build_half(int* half)
+{
+    constexpr int N = N1 * N2;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    for (int p0 = 0; p0 < N; p0 += 32) {
+        const int p = p0 + lane;
+        const bool in = p < N && fft::in_half<N1, N2>(p);
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) half[base + __popc(m & ((1u << lane) - 1u))] = p;
+        base += __popc(m);
+    }
+}
+
 __device__ __forceinline__ const float* spec_chip(const SpecSource& s, long long pair0, int b)
 {
     return s.chip + (s.chip_off ? s.chip_off[pair0 + b] : (long long)b * s.chip_step);
@@ -341,6 +358,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
     float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
     int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
+    int* half = reinterpret_cast<int*>(ssm + g.off_half);
     double* red = reinterpret_cast<double*>(ssm + g.off_red);
     float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
     float* G = reinterpret_cast<float*>(ssm + g.off_gam);
@@ -381,6 +399,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         tw[k] = __ldg(tw_g + k);
         neg[k] = fft::neg_pos<N1, N2>(k);
     }
+    if (warp == 0) build_half<N1, N2>(half);
     cp_async_wait_all();
     __syncthreads();
 
@@ -453,7 +472,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float bv = -INFINITY;
     int bi = INT_MAX;
     int flagged = 0;
-    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, centre, tid, kThreads, BlockSync{},
+    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, half, centre, tid, kThreads, BlockSync{},
                                 [&](int u, int v, float2 val) {
                                     if (v < C) {
                                         const int idx = u * C + v;
@@ -714,6 +733,7 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
     float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
     float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
     int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
+    int* half = reinterpret_cast<int*>(ssm + g.off_half);
     double* red = reinterpret_cast<double*>(ssm + g.off_red);
     float* Zf = reinterpret_cast<float*>(Z);
     const long long cs = src.chip_stride, ws = src.win_stride;
@@ -746,6 +766,7 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
         tw[q] = __ldg(tw_g + q);
         neg[q] = fft::neg_pos<N1, N2>(q);
     }
+    if (warp == 0) build_half<N1, N2>(half);
     cp_async_wait_all();
     __syncthreads();
 
@@ -786,9 +807,9 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
             if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = cr[j][i];
         }
     __syncthreads();
-    // the last inverse step writes its outputs back where it read them (in place), so the
-    // numerators of placement row u sit in tile row u
-    fft::correlate_tile<N1, N2>(Z, RS, S, C, tw, neg, centre, tid, kThreads, BlockSync{},
+    // the last inverse step hands placement row u to the store, which puts it in tile row u (no
+    // later step reads those rows), so the numerators need no buffer beside the tile
+    fft::correlate_tile<N1, N2>(Z, RS, S, C, tw, neg, half, centre, tid, kThreads, BlockSync{},
                                 [&](int u, int v, float2 val) { Z[u * RS + v] = val; });
     const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
     float* out = part + ((long long)b * K + k) * C * C;
