@@ -506,6 +506,7 @@ struct ampcor_handle {
     bool refine_fft = false;
     float* d_tw_refine = nullptr;
     bool refine_big = false;
+    bool refine_strips = false;  // every refinement through the strip kernel (AMPCOR_REFINE_STRIPS)
     float2* d_upy = nullptr;
     long long upy_len = 0;
     // blocked spectral stages (coarse, fine): chip statistics, placement statistics, partial
@@ -945,12 +946,12 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
             const float2* tw = reinterpret_cast<const float2*>(h->d_tw_refine);
             CK(h, launch_spec_refine(h->R, n, st, src.ref_base, src.ref_off, src.ref_stride, nullptr, c0,
                                      n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0,
-                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy),
+                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy, h->refine_strips),
                "launching the chip refinement");
             CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
                                      c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
                                      h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf,
-                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy),
+                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy, h->refine_strips),
                "launching the window refinement");
         } else {
             refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
@@ -1093,7 +1094,11 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         const bool big_w = !small_w && spec_refine_big_supported(h->E, h->f, sm_w);
         h->refine_fft = (small_c || big_c) && (small_w || big_w) &&
                         !(std::getenv("AMPCOR_REFINE_TAPS") && interp_ok);
-        h->refine_big = h->refine_fft && (big_c || big_w);
+        int sm_sc = 0, sm_sw = 0;
+        h->refine_strips = h->refine_fft && std::getenv("AMPCOR_REFINE_STRIPS") &&
+                           std::atoi(std::getenv("AMPCOR_REFINE_STRIPS")) == 1 &&
+                           spec_refine_big_supported(h->R, h->f, sm_sc) && spec_refine_big_supported(h->E, h->f, sm_sw);
+        h->refine_big = h->refine_fft && (big_c || big_w || h->refine_strips);
         h->upy_len = std::max((long long)h->R * h->Rf, (long long)h->E * h->Wf);
         const bool direct_c = plan_spec(h->R, h->W, h->spc, serr);
         const bool coarse_ok = direct_c || plan_spec_blocked(h->R, h->W, h->bc, serr);

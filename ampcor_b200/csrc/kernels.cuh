@@ -279,15 +279,16 @@ int spec_next_length(int w);
 cudaError_t spec_set_smem_limits();
 // refinement by zero-padded FFT for an N x N tile and factor f, when compiled (smem: its bytes)
 bool spec_refine_supported(int n, int f, int& smem);
-// refinement of tiles too large for one CTA's shared memory (N in 96 .. 160, f = 2): rows and
-// columns in strips through a per-pair buffer of N x 2N complex samples (ybuf, blocks of them)
+// refinement in strips through a per-pair buffer of N x 2N complex samples in global memory
+// (ybuf, blocks of them): tiles too large for one CTA's shared memory (N in 96 .. 160, f = 2), and
+// with `strips` the shorter compiled lengths too (less shared memory, more CTAs per SM)
 bool spec_refine_big_supported(int n, int f, int& smem);
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
                                long long refined_stride, long long out_off, int deramp,
-                               float2* ybuf);
+                               float2* ybuf, bool strips);
 
 // blocked spectral correlation (windows too large for one tile; see spectral.cu): per chunk of
 // pairs the chip statistics, the placement statistics when no raster gives them, the partial

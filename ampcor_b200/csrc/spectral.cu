@@ -1053,8 +1053,13 @@ spec_refine_big_kernel(const float2* base, const long long* off, long long strid
     }
 }
 
-// refinement lengths too large for fft_upsample: N, N1, N2, F1, F2 (F = 2 N)
+// refinement lengths of the strip kernel: N, N1, N2, F1, F2 (F = 2 N); 96 and up are too large for
+// fft_upsample, the shorter ones may run either way (AMPCOR_REFINE_STRIPS)
 #define AMPCOR_REFINE_BIG(X) \
+    X(32, 4, 8, 8, 8)        \
+    X(48, 6, 8, 8, 12)       \
+    X(64, 8, 8, 8, 16)       \
+    X(80, 8, 10, 10, 16)     \
     X(96, 8, 12, 12, 16)     \
     X(120, 8, 15, 15, 16)    \
     X(128, 8, 16, 16, 16)    \
@@ -1253,10 +1258,10 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
                                long long pair0, long long pairs, const long long* valid,
                                const float2* twn, const float2* twf, float* refined,
                                long long refined_stride, long long out_off, int deramp,
-                               float2* ybuf)
+                               float2* ybuf, bool strips)
 {
     int small_smem = 0;
-    if (!spec_refine_supported(n, 2, small_smem) && ybuf) {
+    if ((strips || !spec_refine_supported(n, 2, small_smem)) && ybuf) {
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                              \
         if (n == NN) {                                                                                  \
             if (deramp)                                                                                 \

@@ -604,10 +604,25 @@ def serving_run(device, args):
     rep["saturation_span_ms"] = 1e3 * max(j.done for j in queued)
     rep["saturation_same_offsets"] = all(np.array_equal(a.offsets, b.offsets) for a, b in zip(jobs, queued))
     rep["geometries"] = len({j.geometry for j in jobs})
+    # the loop at the headline geometry (64 x 64 chips, +-32 px, zoom 8): 24 jobs on rasters of
+    # 1024^2 to 8192^2 queued at once, against the 1.41M pairs/s of one whole job
+    prod = serve.poisson_jobs(24, rate=20.0, seed=8, device=f"cuda:{device}",
+                              sizes=(1024, 2048, 4096, 8192), chips=(64,), margins=(32,), zooms=(8,),
+                              spacing=(33, 64), pinned=False, square=True)
+    for j in prod:
+        j.arrival = 0.0
+    psrv = serve.Server(device=device, slots=3)
+    psrv.warm(prod)
+    psrv.run(prod, realtime=False)
+    prep = serve.latency_report(prod)
+    rep["saturation_headline_geometry_pairs_per_s"] = prep["pairs_per_s"]
+    rep["saturation_headline_geometry_pairs"] = prep["pairs"]
     rep["stream"] = (f"{args.serving_jobs} jobs, Poisson 20 jobs/s (seed 7), square rasters of 1024, "
                      f"2048, 4096 or 8192 px (upload from pinned host memory inside each job's "
                      f"latency), chip 32/64/128, margin 16/32/64, refine 2, zoom 8/16, 3 slots; "
-                     f"saturation: the same jobs queued at once, rasters in device memory")
+                     f"saturation: the same jobs queued at once, rasters in device memory; "
+                     f"headline-geometry saturation: 24 jobs of 64 x 64 chips, +-32 px, zoom 8, "
+                     f"rasters 1024^2-8192^2, queued at once")
     return rep
 
 
