@@ -238,14 +238,14 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     g.off_half = (int)off;  // one position of every Hermitian pair of the spectrum
     off = up(off + (long)(g.N / 2 + 1) * 4, 16);
     g.off_red = (int)off;
-    off += 256;
+    off += 2L * kSpecWarps * 8;
     g.off_inv = (int)off;  // the placement statistics, prefetched with the tiles
     off = up(off + (long)g.C * g.C * 4, 16);
     g.off_gam = (int)off;  // the normalised surface; before the last step, the statistics' scratch
     const long limit = 227L * 1024;
     // column sums (two floats a placement row and window column) past the tile's imaginary parts
     const long over = std::max<long>(0, 2L * g.C * g.W - (long)g.N * g.RS) * 4;
-    g.nseg = std::max(1, kThreads / g.W);
+    g.nseg = std::max(1, kSpecThreads / g.W);
     while (g.nseg > 1 && off + 32L * g.nseg * g.W + over > limit) --g.nseg;
     off = up(off + std::max<long>((long)g.C * g.C * 4, 32L * g.nseg * g.W + over), 16);
     if (off > limit) {
@@ -286,7 +286,7 @@ bool plan_spec_tile(int B, int S, int C, SpecGeom& g)
     g.off_half = (int)off;
     off = up(off + (long)(g.N / 2 + 1) * 4, 16);
     g.off_red = (int)off;
-    off += 256;
+    off += 2L * kSpecWarps * 8;
     g.smem_bytes = (int)off;
     return off <= 227L * 1024;
 }

@@ -21,6 +21,10 @@ namespace ampcor_b200 {
 
 constexpr int kThreads = 512;            // threads per CTA, one CTA per tile pair
 constexpr int kWarps = kThreads / 32;
+// the spectral correlation kernels (one FFT tile per CTA, the tile fills the shared memory): twice
+// the warps at half the registers, so that more warps hide the latency of the transform passes
+constexpr int kSpecThreads = 1024;
+constexpr int kSpecWarps = kSpecThreads / 32;
 constexpr int kMaxVB = 8;                // column blocks of a correlation surface
 constexpr int kSlot = 33;                // row stride of a partial-sum slot (floats)
 constexpr int kStatRows = 8;             // placement rows per window-statistics chunk

@@ -50,7 +50,9 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
 
-// two block-wide FP64 sums in a fixed order (one pair of barriers); every thread gets both
+// two block-wide FP64 sums in a fixed order (one pair of barriers) over a CTA of NW warps; every
+// thread gets both; red holds 2 NW doubles
+template <int NW>
 __device__ void block_sum2(double& a, double& b, double* red)
 {
     a = warp_sum(a);
@@ -64,7 +66,7 @@ __device__ void block_sum2(double& a, double& b, double* red)
     a = 0.0;
     b = 0.0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
+    for (int w = 0; w < NW; ++w) {
         a += red[2 * w];
         b += red[2 * w + 1];
     }
@@ -142,7 +144,7 @@ __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
 // S(v) = sum_{x in [v, v + R)} V(x): S(0) as an FP64 warp sum, the others as S(0) plus an FP32 scan
 // of V(v + R) - V(v) across the lanes.  The phases are bound by instruction issue, so the FP64
 // work and the float-double conversions are kept to a few per column.  Ends with a barrier.
-template <int RS>
+template <int RS, int NT>
 __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, StatSlots vs, double* part,
                                float* invs)
 {
@@ -221,10 +223,10 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
     }
     __syncthreads();
     const double rcells = 1.0 / ((double)R * (double)R);
-    for (int u = warp; u < C; u += 2 * kWarps) {
-        // rows u and u + kWarps; the second is row C - 1 again (not stored) past the end
-        const int uu[2] = {u, min(u + kWarps, C - 1)};
-        const bool keep2 = u + kWarps < C;
+    for (int u = warp; u < C; u += 2 * (NT / 32)) {
+        // rows u and u + (NT / 32); the second is row C - 1 again (not stored) past the end
+        const int uu[2] = {u, min(u + (NT / 32), C - 1)};
+        const bool keep2 = u + (NT / 32) < C;
         double s1[2], s2[2];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -286,9 +288,11 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
 }
 
 // The normalised surface G (C x C in shared memory, formed by the last transform step) -> its
-// first maximum (valid in every thread) and optional copies.  On entry every thread holds the
+// first maximum (valid in every thread) and optional copies; a CTA of NT threads, red holding
+// NT / 32 floats and as many ints.  On entry every thread holds the
 // maximum of the placements it formed whose transform bound is tight, and whether it formed any
 // whose bound is loose (flagged); inv holds 1/sigma_box of the placements (row stride C).
+template <int NT>
 __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const float* inv,
                              float inv_sigma, double mean_c, float ebox, const float* chip,
                              long long cs, const float* win, long long ws, float* out1, float* out2,
@@ -296,14 +300,14 @@ __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const flo
 {
     const int C = g.C, R = g.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
+    block_argmax_n<NT>(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + NT / 32);
     if (__syncthreads_or(flagged)) {
         // direct FP32 numerators where the transform's bound is loose and the value matters: one
         // warp per placement, lanes across the chip columns
         const bool all = out1 || out2;
         float wv = -INFINITY;
         int wi = INT_MAX;
-        for (int idx = warp; idx < C * C; idx += kWarps) {
+        for (int idx = warp; idx < C * C; idx += NT / 32) {
             const int u = idx / C, v = idx - u * C;
             const float inv_box = inv[idx];
             const float e = ebox * inv_box;
@@ -323,10 +327,10 @@ __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const flo
         // every flagged placement that could win has its exact value now; the others stay below
         // the unflagged maximum
         better(bv, bi, wv, wi);
-        block_argmax(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + kWarps);
+        block_argmax_n<NT>(bv, bi, reinterpret_cast<float*>(red), reinterpret_cast<int*>(red) + NT / 32);
     }
     if (out1 || out2) {
-        for (int idx = threadIdx.x; idx < C * C; idx += kThreads) {
+        for (int idx = threadIdx.x; idx < C * C; idx += NT) {
             const float gv = G[idx];
             if (out1) out1[idx] = gv;
             if (out2) out2[idx] = gv;
@@ -335,7 +339,7 @@ __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const flo
 }
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kSpecThreads, 1)
 spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
             InvSource inv, const float2* tw_g, SpecOut out)
 {
@@ -373,16 +377,16 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     // The chip goes to registers (its loads in flight with the window's), the window amplitudes
     // to the real parts of the tile by 4-byte asynchronous copies, zeros to the other real parts.
     // The imaginary parts are the placement statistics' scratch until the chip is stored there.
-    constexpr int JN = (N + kWarps - 1) / kWarps, IN = (N + 31) / 32;
+    constexpr int JN = (N + kSpecWarps - 1) / kSpecWarps, IN = (N + 31) / 32;
     float cr[JN][IN];
 #pragma unroll
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
-            const int y = warp + kWarps * j, x = lane + 32 * i;
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
             cr[j][i] = y < R && x < R ? __ldg(chip + y * cs + x) : 0.0f;
         }
-    for (int y = warp; y < N; y += kWarps) {
+    for (int y = warp; y < N; y += kSpecWarps) {
         float* zr = Zf + 2 * y * RS;
         for (int x = lane; x < N; x += 32) {
             if (y < W && x < W)
@@ -393,9 +397,9 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     }
     // given placement statistics land in shared memory with the window
     if (inv_b)
-        for (int u = warp; u < C; u += kWarps)
+        for (int u = warp; u < C; u += kSpecWarps)
             for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
-    for (int k = tid; k < N; k += kThreads) {
+    for (int k = tid; k < N; k += kSpecThreads) {
         tw[k] = __ldg(tw_g + k);
         neg[k] = fft::neg_pos<N1, N2>(k);
     }
@@ -412,7 +416,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     double acc4[4];
     {
         float sw = 0.0f, sw2 = 0.0f, sc = 0.0f, cc = 0.0f, sc2 = 0.0f;
-        for (int y = warp; y < W; y += kWarps) {
+        for (int y = warp; y < W; y += kSpecWarps) {
             const float2* zr = Z + y * RS;
             for (int x = lane; x < W; x += 32) {
                 const float t = zr[x].x;
@@ -423,7 +427,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         // register slots past the chip hold zeros in every lane: skipped (warp-uniform tests)
 #pragma unroll
         for (int j = 0; j < JN; ++j)
-            if (warp + kWarps * j < R)
+            if (warp + kSpecWarps * j < R)
 #pragma unroll
                 for (int i = 0; i < IN; ++i)
                     if (32 * i < R) {
@@ -438,8 +442,8 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         acc4[1] = sc2;
         acc4[2] = sw;
         acc4[3] = sw2;
-        block_sum2(acc4[0], acc4[1], red);
-        block_sum2(acc4[2], acc4[3], red);
+        block_sum2<kSpecWarps>(acc4[0], acc4[1], red);
+        block_sum2<kSpecWarps>(acc4[2], acc4[3], red);
     }
     const double cells_c = (double)R * (double)R, cells_w = (double)W * (double)W;
     const double mean_c = acc4[0] / cells_c;
@@ -452,7 +456,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     if (!inv_b) {
         double* part = reinterpret_cast<double*>(ssm + g.off_gam);
         const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
-        spec_box_stats<RS>(Z, g, centre.sx, vs, part, invs);
+        spec_box_stats<RS, kSpecThreads>(Z, g, centre.sx, vs, part, invs);
     }
     // the zero-mean chip into the imaginary parts (its FP64 mean off as two floats), zeros around
     // it
@@ -460,7 +464,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
-            const int y = warp + kWarps * j, x = lane + 32 * i;
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
             if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = y < R && x < R ? (cr[j][i] - mc_hi) - mc_lo : 0.0f;
         }
     __syncthreads();
@@ -472,7 +476,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float bv = -INFINITY;
     int bi = INT_MAX;
     int flagged = 0;
-    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, half, centre, tid, kThreads, BlockSync{},
+    fft::correlate_tile<N1, N2>(Z, RS, W, C, tw, neg, half, centre, tid, kSpecThreads, BlockSync{},
                                 [&](int u, int v, float2 val) {
                                     if (v < C) {
                                         const int idx = u * C + v;
@@ -488,7 +492,7 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
-    spec_surface(G, red, g, invs, inv_sigma, mean_c, ebox, chip, cs, win, ws, gam, surf, bv, bi, flagged);
+    spec_surface<kSpecThreads>(G, red, g, invs, inv_sigma, mean_c, ebox, chip, cs, win, ws, gam, surf, bv, bi, flagged);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;
         if (out.stage == 0) {
@@ -715,7 +719,7 @@ spec_tile_stats_kernel(SpecSource src, long long pair0, long long pairs, const l
 // (g.R = B, g.W = B + C - 1, g.C = C), nb blocks per axis.  part: C^2 floats per (pair, block),
 // already scaled; scal: two doubles per (pair, block), s_k sum_k c and |c| |t - s_k|.
 template <int N1, int N2>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kSpecThreads, 1)
 spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
                   int nb, const ChipStat* cstat, const float2* tw_g, float* part, double* scal)
 {
@@ -744,16 +748,16 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
 
     // the block of the chip, centred on the whole chip's mean, to registers; the sub-window to the
     // tile's real parts by asynchronous copies, zeros around it
-    constexpr int JN = (N + kWarps - 1) / kWarps, IN = (N + 31) / 32;
+    constexpr int JN = (N + kSpecWarps - 1) / kSpecWarps, IN = (N + 31) / 32;
     float cr[JN][IN];
 #pragma unroll
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
-            const int y = warp + kWarps * j, x = lane + 32 * i;
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
             cr[j][i] = y < B && x < B ? (__ldg(chip + y * cs + x) - mc_hi) - mc_lo : 0.0f;
         }
-    for (int y = warp; y < N; y += kWarps) {
+    for (int y = warp; y < N; y += kSpecWarps) {
         float* zr = Zf + 2 * y * RS;
         for (int x = lane; x < N; x += 32) {
             if (y < S && x < S)
@@ -762,7 +766,7 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
                 zr[2 * x] = 0.0f;
         }
     }
-    for (int q = tid; q < N; q += kThreads) {
+    for (int q = tid; q < N; q += kSpecThreads) {
         tw[q] = __ldg(tw_g + q);
         neg[q] = fft::neg_pos<N1, N2>(q);
     }
@@ -774,7 +778,7 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
     double a0 = 0.0, a1 = 0.0, a2, a3;
     {
         float sw = 0.0f, sw2 = 0.0f;
-        for (int y = warp; y < S; y += kWarps) {
+        for (int y = warp; y < S; y += kSpecWarps) {
             const float2* zr = Z + y * RS;
             for (int x = lane; x < S; x += 32) {
                 const float t = zr[x].x;
@@ -792,8 +796,8 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
             }
         a2 = sw;
         a3 = sw2;
-        block_sum2(a0, a1, red);
-        block_sum2(a2, a3, red);
+        block_sum2<kSpecWarps>(a0, a1, red);
+        block_sum2<kSpecWarps>(a2, a3, red);
     }
     const double cells_w = (double)S * (double)S;
     const double mean_w = a2 / cells_w;
@@ -803,17 +807,17 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
-            const int y = warp + kWarps * j, x = lane + 32 * i;
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
             if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = cr[j][i];
         }
     __syncthreads();
     // the last inverse step hands placement row u to the store, which puts it in tile row u (no
     // later step reads those rows), so the numerators need no buffer beside the tile
-    fft::correlate_tile<N1, N2>(Z, RS, S, C, tw, neg, half, centre, tid, kThreads, BlockSync{},
+    fft::correlate_tile<N1, N2>(Z, RS, S, C, tw, neg, half, centre, tid, kSpecThreads, BlockSync{},
                                 [&](int u, int v, float2 val) { Z[u * RS + v] = val; });
     const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
     float* out = part + ((long long)b * K + k) * C * C;
-    for (int idx = tid; idx < C * C; idx += kThreads) {
+    for (int idx = tid; idx < C * C; idx += kSpecThreads) {
         const int u = idx / C, v = idx - u * C;
         out[idx] = Z[u * RS + v].x * scale;
     }
@@ -884,8 +888,8 @@ spec_reduce_kernel(SpecSource src, long long pair0, long long pairs, const long 
     const float* win = spec_win(src, pair0, blockIdx.x);
     float* surf = out.surfaces ? out.surfaces + (size_t)p * CC : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * CC : nullptr;
-    spec_surface(G, red, g, invs, inv_sigma, cst.mean, ebox, chip, src.chip_stride, win, src.win_stride, gam,
-                 surf, bv, bi, flagged);
+    spec_surface<kThreads>(G, red, g, invs, inv_sigma, cst.mean, ebox, chip, src.chip_stride, win,
+                           src.win_stride, gam, surf, bv, bi, flagged);
     if (tid == 0) {
         const int u = bi / C, v = bi - u * C;
         if (out.stage == 0) {
@@ -1360,7 +1364,7 @@ cudaError_t launch_spec_block(const SpecGeom& tile, int nb, unsigned blocks, cud
 {
 #define AMPCOR_SPEC_CASE(NN, A, B)                                                                   \
     if (tile.N == NN) {                                                                              \
-        spec_block_kernel<A, B><<<blocks, kThreads, tile.smem_bytes, st>>>(src, pair0, pairs, valid, \
+        spec_block_kernel<A, B><<<blocks, kSpecThreads, tile.smem_bytes, st>>>(src, pair0, pairs, valid, \
                                                                            tile, nb, cstat, tw, part, scal); \
         return cudaGetLastError();                                                                   \
     }
@@ -1391,7 +1395,7 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 {
 #define AMPCOR_SPEC_CASE(NN, A, B)                                                              \
     if (g.N == NN) {                                                                            \
-        spec_kernel<A, B><<<blocks, kThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g, \
+        spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g, \
                                                                   inv, tw, out);                \
         return cudaGetLastError();                                                              \
     }

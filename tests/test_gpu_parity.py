@@ -97,6 +97,21 @@ def test_plain_512_parity(form):
 
 
 @pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("dc", [30.0, 300.0])
+def test_large_dc_offset_parity(form, dc):
+    # a strong steady return under the speckle (amplitudes near dc, variations of order 1): the
+    # window variances S2 - S1^2 / R^2 cancel in proportion to dc^2, the stress the FP64 box
+    # statistics and the centred in-kernel column sums are there for
+    base = synth.plain_512()
+    w = synth.Workload(f"plain_512_dc{int(dc)}", (base.ref + np.complex64(dc)).astype(np.complex64),
+                       (base.tgt + np.complex64(dc)).astype(np.complex64), base.ulhc, base.centres,
+                       32, 8, 2, 4, 4, base.truth)
+    gpu = run_device(w, form=form)
+    rep = check_parity(w, w.ulhc, gpu, f"plain_512 + {dc} {form}", orc=oracle_of(w, key=w.name))
+    assert rep["pairs_checked"] == 64
+
+
+@pytest.mark.parametrize("form", FORMS)
 def test_golden_plain_512_on_gpu(form):
     import os
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "plain_512.npz"))
