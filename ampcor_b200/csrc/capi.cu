@@ -361,7 +361,7 @@ bool plan_zoom_tc(int Cf, int z, ZoomTcGeom& g)
     g.off_bar = (int)off;
     off += 48;  // five mbarriers (the fifth is waited on only by failure-detection tests)
     g.off_misc = (int)off;
-    off += 128;
+    off += 256;  // tensor-memory address, error flag, and the block maximum's per-warp slots
     g.smem_bytes = (int)off;
     return off <= 227L * 1024;
 }
@@ -772,7 +772,7 @@ int launch_zoom(ampcor_handle* h, long long c0, unsigned n, const PairSource& sr
     const int compat = (h->prm.flags & AMPCOR_FLAG_REF_COMPAT) ? 1 : 0;
     if (h->zoom_tc) {
         const unsigned blocks = std::min<unsigned>(n, 148u);
-        tc_zoom_kernel<<<blocks, 256, h->ztc.smem_bytes, st>>>(
+        tc_zoom_kernel<<<blocks, kTcZoomThreads, h->ztc.smem_bytes, st>>>(
             h->d_gam, c0, n, src.ref_off, h->ztc, h->d_zoom_uhl, h->d_coarse, h->d_coarse_peak,
             h->d_fine_out, h->M, h->f, h->m, compat, offsets, diag, h->d_tc_err, h->inject_timeouts > 0 ? 1 : 0);
     } else {

@@ -260,6 +260,23 @@ HD void fwd_a(float2* base, int es, int n2, const float2* tw)
     for (int k1 = 0; k1 < N1; ++k1) base[(N2 * k1 + n2) * es] = a[k1];
 }
 
+// fwd_a with a constant m taken off every input on the way in
+template <int N1, int N2>
+HD void fwd_a_minus(float2* base, int es, int n2, const float2* tw, float2 m)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        const float2 v = base[(N2 * n1 + n2) * es];
+        a[n1] = make_float2(v.x - m.x, v.y - m.y);
+    }
+    Dft<N1, -1>::run(a);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[n2 * k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) base[(N2 * k1 + n2) * es] = a[k1];
+}
+
 // Centring applied on the way in (the first pass over the rows): element n of row y gets sx
 // taken off its real part when y < wx and n < wx.  A zero shift leaves the tile as it is.
 struct Centre {
@@ -308,6 +325,21 @@ HD void inv_a(float2* base, int es, int n2, const float2* tw)
     Dft<N1, 1>::run(a);
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) base[(N2 * n1 + n2) * es] = a[n1];
+}
+
+// inv_a that writes back only the outputs n < lim (the rows a later step reads)
+template <int N1, int N2>
+HD void inv_a_lim(float2* base, int es, int n2, const float2* tw, int lim)
+{
+    float2 a[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) a[k1] = base[(N2 * k1 + n2) * es];
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmulc(a[k1], tw[n2 * k1]);
+    Dft<N1, 1>::run(a);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1)
+        if (N2 * n1 + n2 < lim) base[(N2 * n1 + n2) * es] = a[n1];
 }
 
 // inv_a whose natural-order outputs go to store(n, value) instead of back into the tile
@@ -427,6 +459,54 @@ HD void half_positions(int* out)
         if (in_half<N1, N2>(p)) out[c++] = p;
 }
 
+// One task of the pass that joins the columns' forward step B, the correlation spectrum and the
+// inverse's step B on the Hermitian half.  The group of column x at positions N2 k1 + k2 holds
+// the frequencies whose negatives sit in column xn = neg_pos(x) at positions N2 k1n + k2n, with
+// k1n = -k1 mod N1 and k2n = -k2 mod N2 when k1 = 0, N2 - 1 - k2 otherwise (pos_of, freq_at).  The
+// task takes both groups through the forward step B, forms the cell pairs in registers, and writes
+// the inverse step B of column x back into the group (of both groups when x is its own partner:
+// the columns of frequencies 0 and N/2).  Every (column, group) belongs to one task, so the pass
+// runs in place without a barrier between its steps.
+template <int N1, int N2, bool K0>
+HD void spectrum_groups(float2* Z, int RS, int x, int xn, int k1)
+{
+    const int k1n = K0 ? 0 : N1 - k1;
+    const bool self_col = x == xn, self = self_col && k1 == k1n;
+    float2 a[N2], b[N2];
+#pragma unroll
+    for (int j = 0; j < N2; ++j) a[j] = Z[(N2 * k1 + j) * RS + x];
+    Dft<N2, -1>::run(a);
+    if (self) {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) b[j] = a[j];
+    } else {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) b[j] = Z[(N2 * k1n + j) * RS + xn];
+        Dft<N2, -1>::run(b);
+    }
+    // s: the spectrum of column x, group k1; b becomes that of the partner group (x's own group
+    // k1n when the column is its own partner)
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+        const int k2n = K0 ? (N2 - k2) % N2 : N2 - 1 - k2;
+        const float2 c = corr_cell(a[k2], b[k2n]);
+        a[k2] = c;
+    }
+    if (self_col && !self) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            const int k2n = K0 ? (N2 - k2) % N2 : N2 - 1 - k2;
+            b[k2n] = make_float2(a[k2].x, -a[k2].y);
+        }
+        Dft<N2, 1>::run(b);
+#pragma unroll
+        for (int j = 0; j < N2; ++j) Z[(N2 * k1n + j) * RS + x] = b[j];
+    }
+    Dft<N2, 1>::run(a);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) Z[(N2 * k1 + j) * RS + x] = a[j];
+}
+
 // ---- the 2-D correlation of one tile pair -------------------------------------------------
 //
 // Z: an N x N tile (row stride RS, odd, so that lanes walking rows or columns hit distinct banks)
@@ -461,35 +541,23 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
         fwd_a<N1, N2>(Z + x, RS, n2, tw);
     }
     sync();
-    for (int t = tid; t < N * N1; t += nt) {
-        const int x = t % N, k1 = t / N;
-        step_b<N1, N2, -1>(Z + x, RS, k1);
-    }
-    sync();
-    // correlation spectrum, one thread per cell pair (k, -k)
-    for (int t = tid; t < N * N; t += nt) {
-        const int py = t / N, px = t - py * N;
-        const int qy = neg[py], qx = neg[px];
-        const int l2 = qy * N + qx;
-        if (t <= l2) {
-            const float2 a = Z[py * RS + px];
-            const float2 b = Z[qy * RS + qx];
-            const float2 c = corr_cell(a, b);
-            Z[py * RS + px] = c;
-            if (t != l2) Z[qy * RS + qx] = make_float2(c.x, -c.y);
-        }
-    }
-    sync();
-    // inverse along the columns of the Hermitian half
+    // the columns' forward step B, the correlation spectrum and the inverse's step B on the
+    // columns of the Hermitian half, one task per pair of column groups
     constexpr int NH = half_count<N1, N2>();
     for (int t = tid; t < NH * N1; t += nt) {
         const int c = t % NH, k1 = t / NH;
-        step_b<N1, N2, 1>(Z + half[c], RS, k1);
+        const int x = half[c], xn = neg[x];
+        if (x == xn && k1 > (N1 - k1) % N1) continue;  // done by the task of the partner group
+        if (k1 == 0)
+            spectrum_groups<N1, N2, true>(Z, RS, x, xn, k1);
+        else
+            spectrum_groups<N1, N2, false>(Z, RS, x, xn, k1);
     }
     sync();
+    // (only the placement rows are read from here on)
     for (int t = tid; t < NH * N2; t += nt) {
         const int c = t % NH, n2 = t / NH;
-        inv_a<N1, N2>(Z + half[c], RS, n2, tw);
+        inv_a_lim<N1, N2>(Z + half[c], RS, n2, tw, rows_out);
     }
     sync();
     const int np = (rows_out + 1) / 2;

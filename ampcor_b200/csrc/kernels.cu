@@ -126,6 +126,33 @@ __device__ double chip_stats(float* chip, const NccGeom& g, double* red)
     return ss > 0.0 ? 1.0 / sqrt(ss) : 0.0;
 }
 
+// The staged window less its smallest sample c: sum r' (t - c) = sum r' t since sum r' = 0.
+// Amplitudes are non-negative, so 0 <= t - c <= t: no term grows, a window that holds a zero
+// sample is left as it is (an all-zero box keeps a numerator of exactly zero), and under a strong
+// steady return the FP32 numerators round on the window's variation, not on its level.  red:
+// kWarps doubles; ends with a barrier.
+__device__ void shift_window(float* win, const NccGeom& g, double* red)
+{
+    float m = INFINITY;
+    for (int idx = threadIdx.x; idx < g.W * g.W; idx += kThreads) {
+        const int r = idx / g.W, col = idx - r * g.W;
+        m = fminf(m, win[r * g.S + col]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(kFull, m, o));
+    float* rf = reinterpret_cast<float*>(red);
+    if ((threadIdx.x & 31) == 0) rf[threadIdx.x >> 5] = m;
+    __syncthreads();
+    float c = rf[0];
+    for (int w = 1; w < kWarps; ++w) c = fminf(c, rf[w]);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < g.W * g.W; idx += kThreads) {
+        const int r = idx / g.W, col = idx - r * g.W;
+        win[r * g.S + col] -= c;
+    }
+    __syncthreads();
+}
+
 // the correlation surface gamma (C x C) from the staged window, the zero-mean chip and the
 // placement statistics; the window region is reused for the partial sums
 __device__ void ncc_surface(const NccGeom& g, float* smem, float inv_sigma)
@@ -259,6 +286,15 @@ __device__ void interp_tile(const float2* __restrict__ src, long long src_stride
     __syncthreads();
     // the row-interpolated buffer is free until the rows are written: the deramp's scratch
     if (deramp) deramp_tile(X, NS, N, reinterpret_cast<double*>(Y));
+    // the tile's mean off before the interpolation (which keeps a constant as it is), back on
+    // with the amplitudes, so that the FP32 sums round on the tile's variation
+    const float2 mu = tile_mean<false, false>(X, NS, N, 0.0f, 0.0f, reinterpret_cast<double*>(Y));
+    for (int idx = threadIdx.x; idx < N * N; idx += kThreads) {
+        const int r = idx / N, c = idx - r * N;
+        const float2 z = X[r * NS + c];
+        X[r * NS + c] = make_float2(z.x - mu.x, z.y - mu.y);
+    }
+    __syncthreads();
 
     // rows: Y[e][f q] = X[e][q], Y[e][f q + s] interpolated
     for (int idx = threadIdx.x; idx < N * N; idx += kThreads) {
@@ -287,7 +323,8 @@ __device__ void interp_tile(const float2* __restrict__ src, long long src_stride
     for (int idx = threadIdx.x; idx < N * F; idx += kThreads) {
         const int q = idx / F, p = idx - q * F;
         const float2 y = Y[q * YS + p];
-        out[(long long)(f * q) * F + p] = sqrtf(y.x * y.x + y.y * y.y);
+        const float re = y.x + mu.x, im = y.y + mu.y;
+        out[(long long)(f * q) * F + p] = sqrtf(re * re + im * im);
     }
     const int npb = (F + 31) / 32;
     for (int t = warp; t < (f - 1) * nqb * npb; t += kWarps) {
@@ -302,8 +339,10 @@ __device__ void interp_tile(const float2* __restrict__ src, long long src_stride
             for (int q = 0; q < kQB; ++q) ar[q] = ai[q] = 0.0f;
             interp_ring(taps + (s - 1) * ig.taps_len + q0, Y + (N - 1) * YS + p, -YS, N, ar, ai);
 #pragma unroll
-            for (int q = 0; q < kQB; ++q)
-                out[(long long)(f * (q0 + q) + s) * F + p] = sqrtf(ar[q] * ar[q] + ai[q] * ai[q]);
+            for (int q = 0; q < kQB; ++q) {
+                const float re = ar[q] + mu.x, im = ai[q] + mu.y;
+                out[(long long)(f * (q0 + q) + s) * F + p] = sqrtf(re * re + im * im);
+            }
         }
     }
     __syncthreads();
@@ -451,7 +490,7 @@ coarse_kernel(PairSource src, long long pair0, long long pairs, NccGeom g, int m
     window_stats(win, g, inv, reinterpret_cast<double*>(chip));
     stage_cplx(chip, g.R, g.R, g.CS, src.ref_base + roff, src.ref_stride);
     const double inv_sigma = chip_stats(chip, g, red);
-    __syncthreads();
+    shift_window(win, g, red);
     ncc_surface(g, smem, (float)inv_sigma);
 
     if (surfaces) {
@@ -522,7 +561,7 @@ fine_kernel(const float* refined, long long refined_stride, long long pair0, lon
     window_stats(win, g, inv, reinterpret_cast<double*>(chip));
     stage_real(chip, g.R, g.R, g.CS, rchip);
     const double inv_sigma = chip_stats(chip, g, red);
-    __syncthreads();
+    shift_window(win, g, red);
     ncc_surface(g, smem, (float)inv_sigma);
 
     if (surfaces) {

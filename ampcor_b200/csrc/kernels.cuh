@@ -21,9 +21,10 @@ namespace ampcor_b200 {
 
 constexpr int kThreads = 512;            // threads per CTA, one CTA per tile pair
 constexpr int kWarps = kThreads / 32;
-// the spectral correlation kernels (one FFT tile per CTA, the tile fills the shared memory): twice
-// the warps at half the registers, so that more warps hide the latency of the transform passes
-constexpr int kSpecThreads = 1024;
+// threads of the spectral correlation kernels (one FFT tile per CTA, the tile fills the shared
+// memory): 16 warps at up to 128 registers.  32 warps at 64 registers ran slower on B200 (coarse
+// 2.42 against 2.27 ms, fine 3.90 against 3.73 ms per production job).
+constexpr int kSpecThreads = 512;
 constexpr int kSpecWarps = kSpecThreads / 32;
 constexpr int kMaxVB = 8;                // column blocks of a correlation surface
 constexpr int kSlot = 33;                // row stride of a partial-sum slot (floats)
@@ -197,6 +198,9 @@ struct ZoomTcGeom {
     int smem_bytes;
 };
 
+// threads of tc_zoom_kernel: four warps per tensor-memory lane quarter
+constexpr int kTcZoomThreads = 512;
+
 // zoom of the refined surfaces of a chunk on the tensor cores; same outputs as zoom_kernel.
 // uhl: the hi and lo planes of U, contiguous.  One CTA per SM walks the pairs.  stall != 0 (a
 // failure-detection test) makes every CTA's first wait on a barrier nothing completes: the
@@ -222,6 +226,9 @@ struct SpecGeom {
     // tile, right after the partial sums
     int nseg;
     int smem_bytes;
+    // CTAs of the kernel resident on the device at once (set at launch): each CTA prefetches into
+    // L2 the tiles of the pair this far ahead, the one that will take its place; 0 turns it off
+    int ahead;
 };
 
 // float amplitude tiles of chunk-local pair b (global pair pair0 + b): at base + off[pair0 + b]

@@ -100,6 +100,19 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
     return s.win + (s.win_off ? s.win_off[pair0 + b] : (long long)b * s.win_step);
 }
 
+// every 128-byte line of a rows x cols float tile (rows `stride` floats apart) into L2, one
+// prefetch per line spread over the block; each row's last element is fetched too, for the line
+// a row that does not start on a line boundary ends in, so every address stays inside the tile
+__device__ __forceinline__ void prefetch_tile(const float* t, int rows, int cols, long long stride)
+{
+    const int lpr = (cols + 31) / 32 + 1;
+    for (int k = threadIdx.x; k < rows * lpr; k += blockDim.x) {
+        const int y = k / lpr, l = k - y * lpr;
+        const int x = 32 * l < cols ? 32 * l : cols - 1;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(t + (long long)y * stride + x));
+    }
+}
+
 // The transform's error on a numerator is a small multiple of eps |r'| |t'| (|.|: Euclidean norms
 // of the zero-mean chip and the centred window; below 1.4e-7 |r'| |t'| over the compiled lengths
 // in host runs against FP64 sums), so its error on gamma is bounded by kSpecErr |t'| / sigma_box.
@@ -312,11 +325,18 @@ __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const flo
             const float inv_box = inv[idx];
             const float e = ebox * inv_box;
             if (!(e > kSpecTol) || !(all || G[idx] + e >= bv)) continue;
+            // the window less the box's own mean (sum r' (t - c) = sum r' t for any constant c):
+            // the FP32 sums round on the box's variation, not on its level, and an all-zero box
+            // keeps a numerator of exactly zero
+            float sb = 0.0f;
+            for (int i = 0; i < R; ++i)
+                for (int j = lane; j < R; j += 32) sb += __ldg(win + (u + i) * ws + v + j);
+            const float wsh = (float)(warp_sum((double)sb) / ((double)R * (double)R));
             float acc = 0.0f;
             for (int i = 0; i < R; ++i)
                 for (int j = lane; j < R; j += 32) {
                     const float rp = (float)((double)__ldg(chip + i * cs + j) - mean_c);
-                    acc = fmaf(rp, __ldg(win + (u + i) * ws + v + j), acc);
+                    acc = fmaf(rp, __ldg(win + (u + i) * ws + v + j) - wsh, acc);
                 }
             const double num = warp_sum((double)acc);
             const float gv = (float)num * inv_box * inv_sigma;
@@ -404,22 +424,34 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         neg[k] = fft::neg_pos<N1, N2>(k);
     }
     if (warp == 0) build_half<N1, N2>(half);
+    // the tiles of the pair that takes this CTA's place, into L2 while this one computes
+    if (g.ahead > 0 && (long long)blockIdx.x + g.ahead < pairs) {
+        const int bn = (int)(blockIdx.x + g.ahead);
+        if (valid[pair0 + bn] >= 0) {
+            prefetch_tile(spec_chip(src, pair0, bn), R, R, cs);
+            prefetch_tile(spec_win(src, pair0, bn), W, W, ws);
+        }
+    }
     cp_async_wait_all();
     __syncthreads();
 
-    // One sweep of sums, combined across the block in FP64: the window's sum and sum of squares,
-    // the chip's sum (compensated) and sum of squares, each thread over a few dozen samples in
-    // FP32.  They give the chip mean, 1/|r'| with |r'|^2 = sum r^2 - R^2 mean^2 (refStats.cu:118-302)
-    // and |t'| of the centred window.  The chip mean comes off as the chip goes into the tile (two
-    // floats, so that r' carries the FP64 mean), the window mean as the first transform pass reads
-    // the tile; the latter only conditions the transform and |t'| only scales its error bound.
+    // Two sweeps of sums, each combined across the block in FP64 (refStats.cu:118-302).  The first
+    // takes the chip's sum (compensated) and, about a pivot k (the window's first sample), the
+    // window's sums of t - k and (t - k)^2; the second the chip's sum of squares with its FP64
+    // mean off (two floats, so that r' carries the FP64 mean; r' stays in the registers): |r'|
+    // exactly, where squares of the uncentred amplitudes would cancel in proportion to the squared
+    // level of a strong steady return.  The window mean comes off as the first transform pass reads
+    // the tile; it only conditions the transform.  |t'|^2 only scales the transform's error bound,
+    // so it is taken as an upper bound: sum (t - k)^2 - (sum (t - k))^2 / W^2 plus 1e-5 sum (t - k)^2,
+    // more than the FP32 rounding of the per-thread sums (at most 50 terms each, 3e-6 relative).
     double acc4[4];
+    const float pk = Z[0].x;
     {
-        float sw = 0.0f, sw2 = 0.0f, sc = 0.0f, cc = 0.0f, sc2 = 0.0f;
+        float sw = 0.0f, sw2 = 0.0f, sc = 0.0f, cc = 0.0f;
         for (int y = warp; y < W; y += kSpecWarps) {
             const float2* zr = Z + y * RS;
             for (int x = lane; x < W; x += 32) {
-                const float t = zr[x].x;
+                const float t = zr[x].x - pk;
                 sw += t;
                 sw2 = fmaf(t, t, sw2);
             }
@@ -431,41 +463,50 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 #pragma unroll
                 for (int i = 0; i < IN; ++i)
                     if (32 * i < R) {
-                        const float r = cr[j][i];
-                        const float yk = r - cc;
+                        const float yk = cr[j][i] - cc;
                         const float tk = sc + yk;
                         cc = (tk - sc) - yk;
                         sc = tk;
-                        sc2 = fmaf(r, r, sc2);
                     }
         acc4[0] = (double)sc - (double)cc;
-        acc4[1] = sc2;
-        acc4[2] = sw;
+        acc4[1] = sw;
         acc4[3] = sw2;
         block_sum2<kSpecWarps>(acc4[0], acc4[1], red);
-        block_sum2<kSpecWarps>(acc4[2], acc4[3], red);
     }
     const double cells_c = (double)R * (double)R, cells_w = (double)W * (double)W;
     const double mean_c = acc4[0] / cells_c;
-    const double ss = acc4[1] - cells_c * mean_c * mean_c;
-    const double mean_w = acc4[2] / cells_w;
-    const double st = fmax(acc4[3] - cells_w * mean_w * mean_w, 0.0);
-    const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
+    const double mean_w = (double)pk + acc4[1] / cells_w;
     const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
     const fft::Centre centre{(float)mean_w, W};
+    {
+        float sc2 = 0.0f;
+#pragma unroll
+        for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int i = 0; i < IN; ++i)
+                if (warp + kSpecWarps * j < R && lane + 32 * i < R) {
+                    const float r = (cr[j][i] - mc_hi) - mc_lo;
+                    cr[j][i] = r;
+                    sc2 = fmaf(r, r, sc2);
+                }
+        acc4[2] = sc2;
+        block_sum2<kSpecWarps>(acc4[2], acc4[3], red);
+    }
+    const double ss = acc4[2];
+    const double st = fmax(acc4[3] - acc4[1] * acc4[1] / cells_w, 0.0) + 1e-5 * acc4[3];
+    const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
     if (!inv_b) {
         double* part = reinterpret_cast<double*>(ssm + g.off_gam);
         const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
         spec_box_stats<RS, kSpecThreads>(Z, g, centre.sx, vs, part, invs);
     }
-    // the zero-mean chip into the imaginary parts (its FP64 mean off as two floats), zeros around
-    // it
+    // the zero-mean chip into the imaginary parts, zeros around it
 #pragma unroll
     for (int j = 0; j < JN; ++j)
 #pragma unroll
         for (int i = 0; i < IN; ++i) {
             const int y = warp + kSpecWarps * j, x = lane + 32 * i;
-            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = y < R && x < R ? (cr[j][i] - mc_hi) - mc_lo : 0.0f;
+            if (y < N && x < N) Zf[2 * (y * RS + x) + 1] = y < R && x < R ? cr[j][i] : 0.0f;
         }
     __syncthreads();
 
@@ -518,22 +559,34 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
 // ------------------------------------------------------------------------------------------
 
 // Upsample the N x N complex tile at src (rows stride apart) by F / N and write its amplitudes
-// (F x F, dense, row stride F) to out: N-point FFTs along the rows; F-point inverses along the
-// rows whose first step reads the N-point spectra padded on the fly (N x F, rows upsampled);
-// N-point FFTs down the columns; then CB columns at a time the F-point inverses, again padding on
-// the fly, and the amplitudes out.  Scaled by 1 / N^2.
-template <int N1, int N2, int F1, int F2, int CB, bool DERAMP>
+// (F x F, dense, row stride F) to out: the tile's 2-D forward transform (N-point FFTs along the
+// rows, then down the N columns), F-point inverses down the N columns that pad each column's
+// spectrum on the fly (F x N), then CB rows at a time the F-point inverses along the rows, again
+// padding on the fly, and the amplitudes out.  Scaled by 1 / N^2.  Transforming both axes forward
+// before padding either costs N + N + N + F transforms, against N + N + F + F when the rows are
+// upsampled first.
+template <int N1, int N2, int F1, int F2>
+struct UpsampleGeom {
+    static constexpr int N = N1 * N2, F = F1 * F2;
+    static constexpr int RSN = N + 1, RSY = N + 1, RSB = F + 1;
+    // output rows per block: the block buffer reuses the tile's space
+    static constexpr int CBX = N * RSN / RSB;
+    static constexpr int CB = CBX < 32 ? CBX : 32;
+    static constexpr int smem = (N * RSN + F * RSY + N + F) * 8;
+    static_assert(CB >= 1, "the row block must fit in the tile's space");
+};
+
+template <int N1, int N2, int F1, int F2, bool DERAMP>
 __device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
                              const float2* __restrict__ twn_g, const float2* __restrict__ twf_g,
                              float* __restrict__ out)
 {
-    constexpr int N = N1 * N2, F = F1 * F2;
-    constexpr int RSN = N + 1, RSF = F + 1, CBS = CB + 1;
-    constexpr int XB = (N * RSN > F * CBS ? N * RSN : F * CBS);
+    using G = UpsampleGeom<N1, N2, F1, F2>;
+    constexpr int N = G::N, F = G::F, RSN = G::RSN, RSY = G::RSY, RSB = G::RSB, CB = G::CB;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float2* X = reinterpret_cast<float2*>(sm);   // the tile, later a block of F-point columns
-    float2* Y = X + XB;                          // rows upsampled: N x F
-    float2* twn = Y + N * RSF;
+    float2* X = reinterpret_cast<float2*>(sm);   // the tile, later a block of F-point rows
+    float2* Y = X + N * RSN;                     // columns upsampled: F x N
+    float2* twn = Y + F * RSY;
     float2* twf = twn + N;
     for (int y = warp; y < N; y += kWarps)
         for (int x = lane; x < N; x += 32) cp_async8_g(X + y * RSN + x, src + y * stride + x);
@@ -541,59 +594,50 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     for (int k = tid; k < F; k += kThreads) twf[k] = __ldg(twf_g + k);
     cp_async_wait_all();
     __syncthreads();
-    // the upsampled-rows buffer is free until the rows are written: the deramp's scratch
+    // the upsampled-columns buffer is free until the columns are written: the deramp's scratch
     if (DERAMP) deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
+    // the tile's mean comes off as the rows are read and back on with the amplitudes
+    const float2 mu = tile_mean<false, false>(X, RSN, N, 0.0f, 0.0f, reinterpret_cast<double*>(Y));
     // rows: forward N
-    for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % N) * RSN, 1, t / N, twn);
+    for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a_minus<N1, N2>(X + (t % N) * RSN, 1, t / N, twn, mu);
     __syncthreads();
     for (int t = tid; t < N * N1; t += kThreads) fft::step_b<N1, N2, -1>(X + (t % N) * RSN, 1, t / N);
     __syncthreads();
-    // rows: inverse F, the first step padding each row's spectrum as it reads it
-    for (int t = tid; t < N * F1; t += kThreads)
-        fft::step_b_pad<N1, N2, F1, F2>(X + (t % N) * RSN, 1, Y + (t % N) * RSF, 1, t / N);
-    __syncthreads();
-    for (int t = tid; t < N * F2; t += kThreads) fft::inv_a<F1, F2>(Y + (t % N) * RSF, 1, t / N, twf);
-    __syncthreads();
     // columns: forward N
-    for (int t = tid; t < F * N2; t += kThreads) fft::fwd_a<N1, N2>(Y + t % F, RSF, t / F, twn);
+    for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a<N1, N2>(X + t % N, RSN, t / N, twn);
     __syncthreads();
-    for (int t = tid; t < F * N1; t += kThreads) fft::step_b<N1, N2, -1>(Y + t % F, RSF, t / F);
+    for (int t = tid; t < N * N1; t += kThreads) fft::step_b<N1, N2, -1>(X + t % N, RSN, t / N);
+    __syncthreads();
+    // columns: inverse F, the first step padding each column's spectrum as it reads it
+    for (int t = tid; t < N * F1; t += kThreads)
+        fft::step_b_pad<N1, N2, F1, F2>(X + t % N, RSN, Y + t % N, RSY, t / N);
+    __syncthreads();
+    for (int t = tid; t < N * F2; t += kThreads) fft::inv_a<F1, F2>(Y + t % N, RSY, t / N, twf);
     __syncthreads();
     const float scale = 1.0f / ((float)N * (float)N);
-    for (int c0 = 0; c0 < F; c0 += CB) {
-        const int nc = F - c0 < CB ? F - c0 : CB;
-        // a block of columns: inverse F (padding on the fly), amplitudes out
+    for (int r0 = 0; r0 < F; r0 += CB) {
+        const int nr = F - r0 < CB ? F - r0 : CB;
+        // a block of rows: inverse F (padding on the fly), amplitudes out
         for (int t = tid; t < CB * F1; t += kThreads) {
-            const int cc = t % CB;
-            if (cc < nc) fft::step_b_pad<N1, N2, F1, F2>(Y + c0 + cc, RSF, X + cc, CBS, t / CB);
+            const int r = t % CB;
+            if (r < nr) fft::step_b_pad<N1, N2, F1, F2>(Y + (r0 + r) * RSY, 1, X + r * RSB, 1, t / CB);
         }
         __syncthreads();
-        // the last step writes the amplitudes of its outputs (rows n of column c0 + cc) straight
-        // to global memory; lanes take consecutive columns, so the stores coalesce
+        // the last step writes the amplitudes of its outputs straight to global memory; lanes take
+        // consecutive outputs of a row, so the stores coalesce
         for (int t = tid; t < CB * F2; t += kThreads) {
-            const int cc = t % CB;
-            if (cc < nc) {
-                float* col = out + c0 + cc;
-                fft::inv_a_store<F1, F2>(X + cc, CBS, t / CB, twf, [&](int n, float2 v) {
-                    const float re = v.x * scale, im = v.y * scale;
-                    col[(long long)n * F] = sqrtf(re * re + im * im);
+            const int r = t / F2, n2 = t - r * F2;
+            if (r < nr) {
+                float* row = out + (long long)(r0 + r) * F;
+                fft::inv_a_store<F1, F2>(X + r * RSB, 1, n2, twf, [&](int n, float2 v) {
+                    const float re = fmaf(v.x, scale, mu.x), im = fmaf(v.y, scale, mu.y);
+                    row[n] = sqrtf(re * re + im * im);
                 });
             }
         }
         __syncthreads();
     }
 }
-
-// shared memory of the upsampling and its column block: 64 columns where the tile needs a whole
-// SM anyway, else 32 (two CTAs per SM fit)
-template <int N1, int N2, int F1, int F2>
-struct UpsampleGeom {
-    static constexpr int N = N1 * N2, F = F1 * F2;
-    static constexpr int smem32 = ((N * (N + 1) > F * 33 ? N * (N + 1) : F * 33) + N * (F + 1) + N + F) * 8;
-    static constexpr int CB = smem32 <= 113 * 1024 ? 32 : 64;
-    static constexpr int smem =
-        ((N * (N + 1) > F * (CB + 1) ? N * (N + 1) : F * (CB + 1)) + N * (F + 1) + N + F) * 8;
-};
 
 // one tile of every pair of a chunk: the chip (coarse == nullptr) or the nudged window; two CTAs
 // per SM where their shared memory allows
@@ -602,18 +646,27 @@ __global__ void __launch_bounds__(kThreads, UpsampleGeom<N1, N2, F1, F2>::smem <
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
-                   long long out_off)
+                   long long out_off, int ahead)
 {
     extern __shared__ __align__(16) unsigned char rsm[];
     if (blockIdx.x >= pairs) return;
     const long long p = pair0 + blockIdx.x;
+    // the tile of the pair that takes this CTA's place (ahead CTAs are resident), into L2
+    if (ahead > 0 && (long long)blockIdx.x + ahead < pairs && valid[p + ahead] >= 0) {
+        const float2* sn = base + off[p + ahead];
+        if (coarse) {
+            const CoarseOut cn = coarse[p + ahead];
+            sn += cn.top * stride + cn.left;
+        }
+        prefetch_tile(reinterpret_cast<const float*>(sn), N1 * N2, 2 * N1 * N2, 2 * stride);
+    }
     if (valid[p] < 0) return;
     const float2* src = base + off[p];
     if (coarse) {
         const CoarseOut co = coarse[p];
         src += co.top * stride + co.left;
     }
-    fft_upsample<N1, N2, F1, F2, UpsampleGeom<N1, N2, F1, F2>::CB, DERAMP>(
+    fft_upsample<N1, N2, F1, F2, DERAMP>(
         src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off);
 }
 
@@ -774,14 +827,17 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
     cp_async_wait_all();
     __syncthreads();
 
-    // FP64 sums of the centred chip block (its sum and sum of squares) and of the sub-window
+    // FP64 sums of the centred chip block (its sum and sum of squares) and of the sub-window about
+    // a pivot k (its first sample): the sums of t - k and (t - k)^2 give its mean and an upper bound
+    // of |t'|^2 (which only scales the error bound), as in spec_kernel
     double a0 = 0.0, a1 = 0.0, a2, a3;
+    const float pk = Z[0].x;
     {
         float sw = 0.0f, sw2 = 0.0f;
         for (int y = warp; y < S; y += kSpecWarps) {
             const float2* zr = Z + y * RS;
             for (int x = lane; x < S; x += 32) {
-                const float t = zr[x].x;
+                const float t = zr[x].x - pk;
                 sw += t;
                 sw2 = fmaf(t, t, sw2);
             }
@@ -800,8 +856,8 @@ spec_block_kernel(SpecSource src, long long pair0, long long pairs, const long l
         block_sum2<kSpecWarps>(a2, a3, red);
     }
     const double cells_w = (double)S * (double)S;
-    const double mean_w = a2 / cells_w;
-    const double st = fmax(a3 - cells_w * mean_w * mean_w, 0.0);
+    const double mean_w = (double)pk + a2 / cells_w;
+    const double st = fmax(a3 - a2 * a2 / cells_w, 0.0) + 1e-5 * a3;
     const fft::Centre centre{(float)mean_w, S};
 #pragma unroll
     for (int j = 0; j < JN; ++j)
@@ -946,8 +1002,8 @@ __device__ void deramp_phases_global(const float2* t, long long stride, int n, d
     __syncthreads();
 }
 
-// Band-limited upsampling of tiles too large to stage whole (N up to 160, F = 2 N): the same
-// transforms as fft_upsample, the rows first, a strip of ST rows at a time (N-point FFTs, F-point
+// Band-limited upsampling of tiles too large to stage whole (N up to 160, F = 2 N): the transforms
+// of fft_upsample in the rows-first order (the mean off as there), a strip of ST rows at a time (N-point FFTs, F-point
 // padded inverses) into a per-pair buffer in global memory (N x F complex, row-major), then the
 // columns of that buffer CB at a time (N-point FFTs, F-point padded inverses, amplitudes out).
 template <int N1, int N2, int F1, int F2>
@@ -989,7 +1045,8 @@ spec_refine_big_kernel(const float2* base, const long long* off, long long strid
     for (int q = tid; q < F; q += kThreads) twf[q] = __ldg(twf_g + q);
     float ps = 0.0f, pl = 0.0f;
     if (DERAMP) deramp_phases_global(src, stride, N, red, ps, pl);
-    __syncthreads();
+    // the tile's mean comes off as the strips are read and back on with the amplitudes
+    const float2 mu = tile_mean<true, DERAMP>(src, stride, N, ps, pl, red);
     // rows, a strip at a time, into the buffer
     for (int r0 = 0; r0 < N; r0 += ST) {
         const int nr = N - r0 < ST ? N - r0 : ST;
@@ -1001,7 +1058,7 @@ spec_refine_big_kernel(const float2* base, const long long* off, long long strid
                 sincosf(fmaf(ps, (float)x, pl * (float)(r0 + y)), &s, &c);
                 z = make_float2(fmaf(z.x, c, z.y * s), fmaf(z.y, c, -z.x * s));
             }
-            X[y * RSN + x] = z;
+            X[y * RSN + x] = make_float2(z.x - mu.x, z.y - mu.y);
         }
         __syncthreads();
         for (int t = tid; t < nr * N2; t += kThreads) fft::fwd_a<N1, N2>(X + (t % nr) * RSN, 1, t / nr, twn);
@@ -1048,7 +1105,7 @@ spec_refine_big_kernel(const float2* base, const long long* off, long long strid
             if (cc < nc) {
                 float* col = out + c0 + cc;
                 fft::inv_a_store<F1, F2>(Y + cc, CBS, t / CB, twf, [&](int n, float2 v) {
-                    const float re = v.x * scale, im = v.y * scale;
+                    const float re = fmaf(v.x, scale, mu.x), im = fmaf(v.y, scale, mu.y);
                     col[(long long)n * F] = sqrtf(re * re + im * im);
                 });
             }
@@ -1257,6 +1314,20 @@ bool spec_refine_big_supported(int n, int f, int& smem)
     return false;
 }
 
+// CTAs of `kernel` resident on the current device at once (SMs x CTAs per SM); 0 when the
+// runtime cannot say, which turns the L2 prefetch off
+template <class K>
+int resident_ctas(K kernel, int threads, int smem)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms * per_sm;
+}
+
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
@@ -1282,12 +1353,15 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
     }
 #define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                           \
     if (n == NN) {                                                                                   \
+        constexpr int smem = UpsampleGeom<A, B, C, D>::smem;                                         \
         if (deramp)                                                                                  \
-            spec_refine_kernel<A, B, C, D, true><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
-                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
+            spec_refine_kernel<A, B, C, D, true><<<blocks, kThreads, smem, st>>>(                    \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off, \
+                resident_ctas(spec_refine_kernel<A, B, C, D, true>, kThreads, smem));                \
         else                                                                                         \
-            spec_refine_kernel<A, B, C, D, false><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem, st>>>( \
-                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
+            spec_refine_kernel<A, B, C, D, false><<<blocks, kThreads, smem, st>>>(                   \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off, \
+                resident_ctas(spec_refine_kernel<A, B, C, D, false>, kThreads, smem));               \
         return cudaGetLastError();                                                                   \
     }
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
@@ -1393,11 +1467,13 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
                         long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out)
 {
-#define AMPCOR_SPEC_CASE(NN, A, B)                                                              \
-    if (g.N == NN) {                                                                            \
-        spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g, \
-                                                                  inv, tw, out);                \
-        return cudaGetLastError();                                                              \
+#define AMPCOR_SPEC_CASE(NN, A, B)                                                               \
+    if (g.N == NN) {                                                                             \
+        SpecGeom ga = g;                                                                         \
+        ga.ahead = resident_ctas(spec_kernel<A, B>, kSpecThreads, g.smem_bytes);                 \
+        spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, ga, \
+                                                                  inv, tw, out);                 \
+        return cudaGetLastError();                                                               \
     }
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
 #undef AMPCOR_SPEC_CASE

@@ -94,6 +94,22 @@ __device__ double block_sum(double v, double* red)
     return s;
 }
 
+// block-wide minimum; every thread gets the same value
+__device__ float block_min(float v, double* red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* r = reinterpret_cast<float*>(red);
+    if (lane == 0) r[warp] = v;
+    __syncthreads();
+    float m = r[0];
+#pragma unroll
+    for (int w = 1; w < kTcWarps; ++w) m = fminf(m, r[w]);
+    __syncthreads();
+    return m;
+}
+
 __device__ __forceinline__ void better(float& bv, int& bi, float v, int i)
 {
     if (v > bv || (v == bv && i < bi)) {
@@ -172,16 +188,24 @@ struct SurfaceMax {
 };
 
 // the numerator of one placement (u, v) as an FP32 dot product (FP64 across threads): the value
-// reported for the maximum, free of the tensor cores' accumulation bias
+// reported for the maximum, free of the tensor cores' accumulation bias.  The window samples go in
+// less the box's own mean (sum r' (t - c) = sum r' t for any constant c): the FP32 sums round on
+// the box's variation, not on its level, and an all-zero box keeps a numerator of exactly zero.
 template <typename Tiles>
 __device__ float placement_gamma(const Tiles& tl, const TcGeom& g, int u, int v, double mean,
                                  float inv_box, float inv_sigma, double* red)
 {
+    float st = 0.0f;
+    for (int idx = threadIdx.x; idx < g.R * g.R; idx += kTcThreads) {
+        const int i = idx / g.R, j = idx - i * g.R;
+        st += tl.win_at(u + i, v + j);
+    }
+    const float shift = (float)(block_sum((double)st, red) / ((double)g.R * (double)g.R));
     float acc = 0.0f;
     for (int idx = threadIdx.x; idx < g.R * g.R; idx += kTcThreads) {
         const int i = idx / g.R, j = idx - i * g.R;
         const float rp = (float)((double)tl.chip_at(i, j) - mean);
-        acc = fmaf(rp, tl.win_at(u + i, v + j), acc);
+        acc = fmaf(rp, tl.win_at(u + i, v + j) - shift, acc);
     }
     const double num = block_sum((double)acc, red);
     return (float)num * inv_box * inv_sigma;
@@ -244,6 +268,14 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
     s2 = block_sum(s2, red);
     const float inv_sigma = s2 > 0.0 ? (float)(1.0 / sqrt(s2)) : 0.0f;
 
+    // the window goes into the split less its smallest sample c: sum r' (t - c) = sum r' t for any
+    // constant c since sum r' = 0.  Amplitudes are non-negative, so 0 <= t - c <= t: no term grows,
+    // a window that holds a zero sample is left as it is (an all-zero box keeps a numerator of
+    // exactly zero), and under a strong steady return the bf16 split rounds on the window's
+    // variation, not on its level
+    float wmin = INFINITY;
+    for (int idx = tid; idx < W * W; idx += kTcThreads) wmin = fminf(wmin, tl.win_at(idx / W, idx % W));
+    const float shift = block_min(wmin, red);
     const uint32_t idesc = instr_desc(g.M, g.N);
     const uint32_t crev_addr = saddr(crev);
     const uint32_t x_addr = saddr(xst);
@@ -299,7 +331,7 @@ __device__ SurfaceMax tc_surface(const Tiles& tl, const TcGeom& g, const float* 
                 for (int idx = pt; idx < NR * g.RB; idx += kProducers) {
                     const int k = idx / g.RB, x = idx - k * g.RB;
                     const int w = si * NR + k;
-                    rb[idx] = (w < W && x < ncols) ? Tiles::amp(raw[(w % kPrefetch) * g.RB + x]) : 0.0f;
+                    rb[idx] = (w < W && x < ncols) ? Tiles::amp(raw[(w % kPrefetch) * g.RB + x]) - shift : 0.0f;
                 }
                 asm volatile("bar.sync 1, %0;" ::"n"(kProducers) : "memory");
                 for (int k = 0; k < NR; ++k) fetch_row((si + 1) * NR + kPrefetch - NR + k);

@@ -14,8 +14,9 @@
 //
 // Operands sit in shared memory as K-major core matrices (8 rows x 16 bytes, no swizzle): row r,
 // element k of a plane at float offset ((r / 8) KC + k / 4) 32 + (r % 8) 4 + k % 4, KC = 16-byte
-// chunks per row.  One CTA of 256 threads per SM walks the pairs of a chunk; lane 0 of warp 7
-// issues the MMAs, all eight warps read accumulators (warps w and w + 4 share lane quarter w).
+// chunks per row.  One CTA of kTcZoomThreads (512) threads per SM walks the pairs of a chunk;
+// lane 0 of the last warp issues the MMAs, all sixteen warps read accumulators (warp w reads lane
+// quarter w % 4; the four warps of a quarter take turns over its columns).
 // Every wait on an mbarrier is bounded; on expiry the kernel records an error, drains its MMAs
 // and frees its tensor memory.
 #include "kernels.cuh"
@@ -26,10 +27,11 @@ namespace ampcor_b200 {
 
 namespace {
 
-constexpr int kZThreads = 256;
-constexpr int kZBatch = 3;  // 16-column accumulator loads in flight per thread
+constexpr int kZThreads = kTcZoomThreads;
+constexpr int kZGroups = kZThreads / 128;  // warps per lane quarter
+constexpr int kZBatch = 3;                 // 16-column accumulator loads in flight per thread
 // the thread that issues every MMA (and the drain after an expired wait): lane 0 of the last
-// warp, whose warp group reads fewer accumulator chunks per unit than the first one
+// warp, whose group reads no more accumulator chunks per unit than the first one
 constexpr int kIssuer = kZThreads - 32;
 
 // accumulator row of this thread in a tile of M rows: M = 128 puts row r in lane r, M = 64 puts
@@ -169,30 +171,27 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
         __syncwarp();
         {
             const bool ok = wait_mma();
-            // row tiles alternate between the two warp groups; each thread writes its row of T^T
-            // into the B planes, split hi / lo
-            for (int mt = group; mt < zt.mtiles; mt += 2) {
+            // row tiles go round the warp groups; each thread writes its row of T^T into the B
+            // planes, split hi / lo
+            for (int mt = group; mt < zt.mtiles; mt += kZGroups) {
                 const int M = (mt == zt.mtiles - 1) ? zt.last_m : 128;
                 const int row = tile_row(M, quarter, lane);
                 const int q = mt * 128 + row;
-                uint32_t r[4][16];
+                const bool keep = ok && row >= 0 && q < Z;
+                const int rowbase = (q >> 3) * KC * 32 + (q & 7) * 4;
+                // one 16-column chunk (four 16-byte K chunks) at a time
+                for (int j = 0; 16 * j < zt.NG; ++j) {
+                    uint32_t r[16];
+                    tmem_ld16_async(tmem + lane_base(quarter) + (uint32_t)(64 * mt + 16 * j), r);
+                    tmem_wait_ld(r);
+                    if (!keep) continue;
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (16 * j < zt.NG) tmem_ld16_async(tmem + lane_base(quarter) + (uint32_t)(64 * mt + 16 * j), r[j]);
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (16 * j < zt.NG) tmem_wait_ld(r[j]);
-                if (ok && row >= 0 && q < Z) {
-                    const int rowbase = (q >> 3) * KC * 32 + (q & 7) * 4;
-#pragma unroll
-                    for (int c4 = 0; c4 < 16; ++c4) {  // KC <= 16: register indices stay static
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int c4 = 4 * j + cc;
                         if (c4 >= KC) break;
                         float h[4], l[4];
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int a = 4 * c4 + k;
-                            split_tf32(__uint_as_float(r[a >> 4][a & 15]), h[k], l[k]);
-                        }
+                        for (int k = 0; k < 4; ++k) split_tf32(__uint_as_float(r[4 * cc + k]), h[k], l[k]);
                         *reinterpret_cast<float4*>(bhi + rowbase + c4 * 32) = make_float4(h[0], h[1], h[2], h[3]);
                         *reinterpret_cast<float4*>(blo + rowbase + c4 * 32) = make_float4(l[0], l[1], l[2], l[3]);
                     }
@@ -235,21 +234,21 @@ tc_zoom_kernel(const float* gam, long long pair0, long long pairs, const long lo
             const int pz = mt * 128 + row;
             const bool live = ok && row >= 0 && pz < Z;
             const uint32_t dbase = tmem + lane_base(quarter) + (uint32_t)((un & 1) * 256);
-            // 16-column chunks alternate between the warp groups, kZBatch loads in flight; a
-            // thread visits its columns in increasing order (parts in order, chunks in order), so
-            // a strict comparison keeps the first maximum
-            for (int c = group; c < pch; c += 2 * kZBatch) {
+            // 16-column chunks go round the warp groups, kZBatch loads in flight; a thread
+            // visits its columns in increasing order (parts in order, chunks in order), so a
+            // strict comparison keeps the first maximum
+            for (int c = group; c < pch; c += kZGroups * kZBatch) {
                 uint32_t r[kZBatch][16];
 #pragma unroll
                 for (int j = 0; j < kZBatch; ++j)
-                    if (c + 2 * j < pch) tmem_ld16_async(dbase + (uint32_t)(16 * (c + 2 * j)), r[j]);
+                    if (c + kZGroups * j < pch) tmem_ld16_async(dbase + (uint32_t)(16 * (c + kZGroups * j)), r[j]);
 #pragma unroll
                 for (int j = 0; j < kZBatch; ++j)
-                    if (c + 2 * j < pch) tmem_wait_ld(r[j]);
+                    if (c + kZGroups * j < pch) tmem_wait_ld(r[j]);
                 if (!live) continue;
 #pragma unroll
                 for (int j = 0; j < kZBatch; ++j) {
-                    const int ci = c + 2 * j;
+                    const int ci = c + kZGroups * j;
                     if (ci >= pch) break;
                     const int q0 = np * zt.npart + 16 * ci;
                     float v[16];

@@ -227,4 +227,44 @@ __device__ inline void deramp_tile(float2* t, int stride, int n, double* red)
     __syncthreads();
 }
 
+// The mean of an n x n complex tile (rows `stride` apart; in shared memory, or in global memory
+// when GLOBAL), with the linear phase ramp (ps, pl) of deramp_tile taken off each sample first
+// when DERAMP.  Band-limited upsampling keeps a constant as it is, so a caller that takes the
+// mean off the tile before its transforms and adds it back to every output gets the same
+// interpolation, with the transforms rounding on the tile's variation instead of on a strong
+// steady return.  FP32 sums per thread, FP64 across the block.  red: 2 kWarps doubles; ends with
+// a barrier.
+template <bool GLOBAL, bool DERAMP>
+__device__ inline float2 tile_mean(const float2* t, long long stride, int n, float ps, float pl, double* red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float sx = 0.0f, sy = 0.0f;
+    for (int k = tid; k < n * n; k += kThreads) {
+        const int y = k / n, x = k - y * n;
+        float2 z = GLOBAL ? __ldg(t + y * stride + x) : t[y * stride + x];
+        if (DERAMP) {
+            float s, c;
+            sincosf(fmaf(ps, (float)x, pl * (float)y), &s, &c);
+            z = make_float2(fmaf(z.x, c, z.y * s), fmaf(z.y, c, -z.x * s));
+        }
+        sx += z.x;
+        sy += z.y;
+    }
+    double a = warp_sum((double)sx), b = warp_sum((double)sy);
+    if (lane == 0) {
+        red[2 * warp] = a;
+        red[2 * warp + 1] = b;
+    }
+    __syncthreads();
+    a = 0.0;
+    b = 0.0;
+    for (int w = 0; w < kWarps; ++w) {
+        a += red[2 * w];
+        b += red[2 * w + 1];
+    }
+    __syncthreads();
+    const double cells = (double)n * (double)n;
+    return make_float2((float)(a / cells), (float)(b / cells));
+}
+
 }  // namespace ampcor_b200

@@ -106,23 +106,27 @@ double check_upsample(std::mt19937& g)
 {
     constexpr int N = N1 * N2, F = F1 * F2, f = F / N;
     std::normal_distribution<double> nd;
-    std::vector<float2> X(N * N), Y(N * F), C(F * F), Out(F * F), twn(N), twf(F);
+    std::vector<float2> X(N * N), Y(F * N), B(F), Out(F * F), twn(N), twf(F);
     for (int m = 0; m < N; ++m) twn[m] = make_float2((float)cos(2 * M_PI * m / N), (float)-sin(2 * M_PI * m / N));
     for (int m = 0; m < F; ++m) twf[m] = make_float2((float)cos(2 * M_PI * m / F), (float)-sin(2 * M_PI * m / F));
     for (auto& v : X) v = make_float2((float)nd(g), (float)nd(g));
     std::vector<float2> X0 = X;
+    // the refinement's order: the 2-D forward transform (rows, then columns), the padded inverse
+    // down the N columns (F x N), then the padded inverse along each of the F rows
     for (int y = 0; y < N; ++y) {
         for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(X.data() + y * N, 1, n2, twn.data());
         for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(X.data() + y * N, 1, k1);
-        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(X.data() + y * N, 1, Y.data() + y * F, 1, k1);
-        for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(Y.data() + y * F, 1, n2, twf.data());
     }
-    for (int x = 0; x < F; ++x) {
-        for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(Y.data() + x, F, n2, twn.data());
-        for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(Y.data() + x, F, k1);
-        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(Y.data() + x, F, C.data() + x, F, k1);
+    for (int x = 0; x < N; ++x) {
+        for (int n2 = 0; n2 < N2; ++n2) fwd_a<N1, N2>(X.data() + x, N, n2, twn.data());
+        for (int k1 = 0; k1 < N1; ++k1) step_b<N1, N2, -1>(X.data() + x, N, k1);
+        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(X.data() + x, N, Y.data() + x, N, k1);
+        for (int n2 = 0; n2 < F2; ++n2) inv_a<F1, F2>(Y.data() + x, N, n2, twf.data());
+    }
+    for (int y = 0; y < F; ++y) {
+        for (int k1 = 0; k1 < F1; ++k1) step_b_pad<N1, N2, F1, F2>(Y.data() + y * N, 1, B.data(), 1, k1);
         for (int n2 = 0; n2 < F2; ++n2)
-            inv_a_store<F1, F2>(C.data() + x, F, n2, twf.data(), [&](int n, float2 v) { Out[n * F + x] = v; });
+            inv_a_store<F1, F2>(B.data(), 1, n2, twf.data(), [&](int n, float2 v) { Out[y * F + n] = v; });
     }
     // direct: out = |A X A^T|, A[i][n] = D_N(i / f - n)
     std::vector<double> A(F * N);
