@@ -226,9 +226,6 @@ struct SpecGeom {
     // tile, right after the partial sums
     int nseg;
     int smem_bytes;
-    // CTAs of the kernel resident on the device at once (set at launch): each CTA prefetches into
-    // L2 the tiles of the pair this far ahead, the one that will take its place; 0 turns it off
-    int ahead;
 };
 
 // float amplitude tiles of chunk-local pair b (global pair pair0 + b): at base + off[pair0 + b]

@@ -100,19 +100,6 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
     return s.win + (s.win_off ? s.win_off[pair0 + b] : (long long)b * s.win_step);
 }
 
-// every 128-byte line of a rows x cols float tile (rows `stride` floats apart) into L2, one
-// prefetch per line spread over the block; each row's last element is fetched too, for the line
-// a row that does not start on a line boundary ends in, so every address stays inside the tile
-__device__ __forceinline__ void prefetch_tile(const float* t, int rows, int cols, long long stride)
-{
-    const int lpr = (cols + 31) / 32 + 1;
-    for (int k = threadIdx.x; k < rows * lpr; k += blockDim.x) {
-        const int y = k / lpr, l = k - y * lpr;
-        const int x = 32 * l < cols ? 32 * l : cols - 1;
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(t + (long long)y * stride + x));
-    }
-}
-
 // The transform's error on a numerator is a small multiple of eps |r'| |t'| (|.|: Euclidean norms
 // of the zero-mean chip and the centred window; below 1.4e-7 |r'| |t'| over the compiled lengths
 // in host runs against FP64 sums), so its error on gamma is bounded by kSpecErr |t'| / sigma_box.
@@ -424,14 +411,6 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
         neg[k] = fft::neg_pos<N1, N2>(k);
     }
     if (warp == 0) build_half<N1, N2>(half);
-    // the tiles of the pair that takes this CTA's place, into L2 while this one computes
-    if (g.ahead > 0 && (long long)blockIdx.x + g.ahead < pairs) {
-        const int bn = (int)(blockIdx.x + g.ahead);
-        if (valid[pair0 + bn] >= 0) {
-            prefetch_tile(spec_chip(src, pair0, bn), R, R, cs);
-            prefetch_tile(spec_win(src, pair0, bn), W, W, ws);
-        }
-    }
     cp_async_wait_all();
     __syncthreads();
 
@@ -646,20 +625,11 @@ __global__ void __launch_bounds__(kThreads, UpsampleGeom<N1, N2, F1, F2>::smem <
 spec_refine_kernel(const float2* base, const long long* off, long long stride,
                    const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
                    const float2* twn, const float2* twf, float* refined, long long refined_stride,
-                   long long out_off, int ahead)
+                   long long out_off)
 {
     extern __shared__ __align__(16) unsigned char rsm[];
     if (blockIdx.x >= pairs) return;
     const long long p = pair0 + blockIdx.x;
-    // the tile of the pair that takes this CTA's place (ahead CTAs are resident), into L2
-    if (ahead > 0 && (long long)blockIdx.x + ahead < pairs && valid[p + ahead] >= 0) {
-        const float2* sn = base + off[p + ahead];
-        if (coarse) {
-            const CoarseOut cn = coarse[p + ahead];
-            sn += cn.top * stride + cn.left;
-        }
-        prefetch_tile(reinterpret_cast<const float*>(sn), N1 * N2, 2 * N1 * N2, 2 * stride);
-    }
     if (valid[p] < 0) return;
     const float2* src = base + off[p];
     if (coarse) {
@@ -1314,20 +1284,6 @@ bool spec_refine_big_supported(int n, int f, int& smem)
     return false;
 }
 
-// CTAs of `kernel` resident on the current device at once (SMs x CTAs per SM); 0 when the
-// runtime cannot say, which turns the L2 prefetch off
-template <class K>
-int resident_ctas(K kernel, int threads, int smem)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return sms * per_sm;
-}
-
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,
@@ -1356,12 +1312,10 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
         constexpr int smem = UpsampleGeom<A, B, C, D>::smem;                                         \
         if (deramp)                                                                                  \
             spec_refine_kernel<A, B, C, D, true><<<blocks, kThreads, smem, st>>>(                    \
-                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off, \
-                resident_ctas(spec_refine_kernel<A, B, C, D, true>, kThreads, smem));                \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
         else                                                                                         \
             spec_refine_kernel<A, B, C, D, false><<<blocks, kThreads, smem, st>>>(                   \
-                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off, \
-                resident_ctas(spec_refine_kernel<A, B, C, D, false>, kThreads, smem));               \
+                base, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off); \
         return cudaGetLastError();                                                                   \
     }
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
@@ -1469,9 +1423,7 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 {
 #define AMPCOR_SPEC_CASE(NN, A, B)                                                               \
     if (g.N == NN) {                                                                             \
-        SpecGeom ga = g;                                                                         \
-        ga.ahead = resident_ctas(spec_kernel<A, B>, kSpecThreads, g.smem_bytes);                 \
-        spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, ga, \
+        spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g,  \
                                                                   inv, tw, out);                 \
         return cudaGetLastError();                                                               \
     }
