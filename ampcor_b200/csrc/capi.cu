@@ -256,6 +256,61 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
     return true;
 }
 
+// The staged form of a stage (spec_staged_kernel), a layout of its own: the tile, then the
+// window's W rows of stage_rs floats at off_stage, which the correlation leaves alone from its
+// inverse column pass on (it keeps its first rows_out + (rows_out + 1) / 2 rows): at the tile's
+// end where the tile has room, else right after the kept rows and on past the tile; the
+// statistics' column sums fit below them.  Tile rows below the staged bytes are written as they
+// are read, the others in pieces of kStagePieces row groups, none of which may reach the staged
+// rows of a later piece.  Rows whose samples may sit off 16-byte boundaries (`dense` false, or W
+// not a multiple of 4) get 3 + W floats rounded up to 16 bytes.
+constexpr int kStagePieces = 3;  // spec_staged_kernel's PJ
+
+bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
+{
+    std::string e;
+    if (!plan_spec(R, W, g, e)) return false;
+    auto up = [](long x, long a) { return (x + a - 1) / a * a; };
+    const int N = g.N, C = g.C;
+    const long row = (long)g.RS * 8, tile = (long)N * row;
+    g.stage_rs = dense && W % 4 == 0 ? W : (W + 6) & ~3;
+    const long stage = (long)W * g.stage_rs * 4;
+    const int np = (C + 1) / 2;
+    const long kept = (long)(C + np <= N ? C + np : C) * row;
+    const long S = up(std::max(kept, tile - stage), 16);
+    if (2L * C * W * 4 > S) return false;
+    const int y0 = (int)std::min<long>(N, S / row) / kSpecWarps * kSpecWarps;
+    const int JN = (N + kSpecWarps - 1) / kSpecWarps;
+    for (int j0 = 0; j0 < JN; j0 += kStagePieces) {
+        const long y1 = (long)std::min(j0 + kStagePieces, JN) * kSpecWarps;
+        if (y1 <= y0 || y1 >= W) continue;
+        if (y1 * row > S + y1 * g.stage_rs * 4) return false;
+    }
+    g.off_stage = (int)S;
+    g.stage_y0 = y0;
+    g.stage_pj = kStagePieces;
+    long off = up(std::max(tile, S + stage), 16);
+    g.off_tw = (int)off;
+    off = up(off + (long)N * 8, 16);
+    g.off_neg = (int)off;
+    off = up(off + (long)N * 4, 16);
+    g.off_half = (int)off;
+    off = up(off + (long)(N / 2 + 1) * 4, 16);
+    g.off_red = (int)off;
+    off += 2L * kSpecWarps * 8;
+    g.off_inv = (int)off;
+    off = up(off + (long)C * C * 4, 16);
+    g.off_gam = (int)off;  // the surface; before the last step, the statistics' partial sums
+    const long limit = 227L * 1024 - 16;
+    g.nseg = std::max(1, kSpecThreads / W);
+    while (g.nseg > 1 && off + 32L * g.nseg * W > limit) --g.nseg;
+    off = up(off + std::max<long>((long)C * C * 4, 32L * g.nseg * W), 16);
+    g.off_bar = (int)off;
+    off += 16;
+    g.smem_staged = off <= limit + 16 ? (int)off : 0;
+    return g.smem_staged > 0;
+}
+
 // A stage of the spectral form whose window is too large for one tile: the chip splits into nb x nb
 // square blocks of side B (B divides R), each block's sub-window (B + C - 1 samples a side) one
 // tile; the largest B whose tile fits is taken.  `full` describes the whole stage for the
@@ -495,6 +550,12 @@ struct ampcor_handle {
     // correlation form (kFormPlain, kFormTensor, kFormSpectral)
     int form = 0;
     SpecGeom spc{}, spf{};
+    // the staged forms of both stages (spec_staged_kernel: one resident CTA per SM, windows
+    // copied in while the previous pair finishes), where planned; sms: the device's
+    // multiprocessors
+    SpecGeom spc_st{}, spf_st{};
+    bool coarse_staged = false, fine_staged = false;
+    int sms = 0;
     // tensor-core zoom (both the tensor-core and the spectral forms), when Zm fits
     bool zoom_tc = false;
     ZoomTcGeom ztc{};
@@ -656,7 +717,8 @@ int ensure_refined(ampcor_handle* h)
     if (h->d_refined) return AMPCOR_OK;
     h->chunk = h->chunk_override ? h->chunk_override : default_chunk();
     h->refined_stride = (long long)h->Rf * h->Rf + (long long)h->Wf * h->Wf;
-    cudaError_t e = cudaMalloc(&h->d_refined, h->chunk * h->refined_stride * sizeof(float));
+    // 16 floats of slack: staged copies round rows out to 16-byte boundaries
+    cudaError_t e = cudaMalloc(&h->d_refined, (h->chunk * h->refined_stride + 16) * sizeof(float));
     if (e != cudaSuccess) {
         h->d_refined = nullptr;
         return scratch_fail(h, std::string("allocating refinement scratch: ") + cudaGetErrorName(e));
@@ -936,9 +998,15 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                                      h->d_part, h->d_scal, co),
                "launching the coarse reduction");
         } else {
-            CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
-                              reinterpret_cast<const float2*>(h->d_tw_c), co),
-               "launching the spectral coarse correlation");
+            // the staged form of the coarse stage takes its statistics from the raster
+            if (h->coarse_staged && r.inv_c.base)
+                CK(h, launch_spec_staged(h->spc_st, (unsigned)h->sms, st, cs, c0, n, src.ref_off, r.inv_c,
+                                         reinterpret_cast<const float2*>(h->d_tw_c), co, h->d_tc_err),
+                   "launching the staged coarse correlation");
+            else
+                CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
+                                  reinterpret_cast<const float2*>(h->d_tw_c), co),
+                   "launching the spectral coarse correlation");
         }
         cudaEvent_t c = mark(h, st);
         keep(h, 0, b, c, h->bc.on ? 2 : 1);
@@ -977,9 +1045,15 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                                      InvSource{h->d_inv_blk, nullptr, 0}, h->d_part, h->d_scal, fo),
                "launching the fine reduction");
         } else {
-            CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
-                              reinterpret_cast<const float2*>(h->d_tw_f), fo),
-               "launching the spectral fine correlation");
+            if (h->fine_staged)
+                CK(h, launch_spec_staged(h->spf_st, (unsigned)h->sms, st, fs, c0, n, src.ref_off,
+                                         InvSource{nullptr, nullptr, 0},
+                                         reinterpret_cast<const float2*>(h->d_tw_f), fo, h->d_tc_err),
+                   "launching the staged fine correlation");
+            else
+                CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
+                                  reinterpret_cast<const float2*>(h->d_tw_f), fo),
+                   "launching the spectral fine correlation");
         }
         cudaEvent_t f = mark(h, st);
         keep(h, 2, e, f, h->bf.on ? 2 : 1);
@@ -1103,6 +1177,16 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         const bool direct_c = plan_spec(h->R, h->W, h->spc, serr);
         const bool coarse_ok = direct_c || plan_spec_blocked(h->R, h->W, h->bc, serr);
         const bool direct_f = coarse_ok && plan_spec(h->Rf, h->Wf, h->spf, serr);
+        // staged forms where they fit (AMPCOR_STAGED=0 keeps spec_kernel); the refined tiles of a
+        // pair are dense rows of one buffer, staged whole when its rows are 16-byte multiples
+        const char* stg = std::getenv("AMPCOR_STAGED");
+        const bool staged_on = !(stg && std::strcmp(stg, "0") == 0);
+        // (the coarse stage stays on spec_kernel: a bulk copy per window row takes longer to issue
+        // than the tail of the previous pair)
+        h->coarse_staged = false;
+        h->fine_staged = staged_on && direct_f &&
+                         plan_spec_staged(h->Rf, h->Wf, h->Rf % 2 == 0 && h->Wf % 2 == 0, h->spf_st) &&
+                         h->spf_st.stage_rs == h->Wf;
         const bool fine_ok = coarse_ok && (direct_f || plan_spec_blocked(h->Rf, h->Wf, h->bf, serr));
         h->spectral_ok = fine_ok && (h->refine_fft || interp_ok);
         if (direct_c || !h->spectral_ok) h->bc = SpecBlocks{};
@@ -1148,6 +1232,8 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
     };
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return cuda_create_fail(e, "creating the worker stream");
+    if ((e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, p->device)) != cudaSuccess)
+        return cuda_create_fail(e, "reading the multiprocessor count");
     // the opt-in limit is per kernel and process-wide: raise it to the device maximum once so
     // that workers of different geometries can coexist
     const int kMaxSmem = 227 * 1024;
@@ -1392,7 +1478,8 @@ int ampcor_synchronize(ampcor_handle* h, void* stream)
     if (tcerr) {
         CK(h, cudaMemsetAsync(h->d_tc_err, 0, sizeof(unsigned int), st), "resetting the error counter");
         CK(h, cudaStreamSynchronize(st), "resetting the error counter");
-        return fail(h, AMPCOR_E_CUDA, std::to_string(tcerr) + " tile pair(s) timed out in the tensor-core pipeline");
+        return fail(h, AMPCOR_E_CUDA, std::to_string(tcerr) +
+                           " tile pair(s) or resident blocks timed out in a bounded device wait");
     }
     if (bad) {
         CK(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned int), st), "resetting the bounds counter");

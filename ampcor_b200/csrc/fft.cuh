@@ -278,22 +278,27 @@ HD void fwd_a_minus(float2* base, int es, int n2, const float2* tw, float2 m)
 }
 
 // Centring applied on the way in (the first pass over the rows): element n of row y gets sx
-// taken off its real part when y < wx and n < wx.  A zero shift leaves the tile as it is.
+// taken off its real part when y < wx and n < wx, and (ci_hi, then ci_lo) off its imaginary part
+// when y < ci and n < ci.  A zero shift leaves the tile as it is.
 struct Centre {
     float sx;
     int wx;
+    float ci_hi = 0.0f, ci_lo = 0.0f;
+    int ci = 0;
 };
 
 template <int N1, int N2>
 HD void fwd_a_centred(float2* row, int y, int n2, const float2* tw, const Centre& c)
 {
     const int lim = y < c.wx ? c.wx : 0;
+    const int ilim = y < c.ci ? c.ci : 0;
     float2 a[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
         const int n = N2 * n1 + n2;
         float2 v = row[n];
         if (n < lim) v.x -= c.sx;
+        if (n < ilim) v.y = (v.y - c.ci_hi) - c.ci_lo;
         a[n1] = v;
     }
     Dft<N1, -1>::run(a);
@@ -518,16 +523,22 @@ HD void spectrum_groups(float2* Z, int RS, int x, int xn, int k1)
 // (circular indices, which never wrap for the placements of a window of at most N samples); the
 // stores of a row go to rows of the tile no later step reads, so store may write into the tile's
 // rows below rows_out.  The tasks of each phase are spread over the nt threads; sync() separates
-// the phases (__syncthreads on the device).
+// the phases (__syncthreads on the device).  cols_done() runs in every thread after the inverse
+// column pass, from which point the correlation touches only the tile's first rows_out +
+// (rows_out + 1) / 2 rows (rows_out where those do not fit in the tile).
 //
 // The inverse runs on the Hermitian half: the columns of the half only (N/2 + 1 of N), after which
 // every placement row is Hermitian along its row; two such rows A, B go through one transform as
 // A + i B (real and imaginary parts of the result), packed into the free rows past rows_out where
 // the tile has them, else each row is completed from its partners and transformed alone.
-template <int N1, int N2, class Sync, class Store>
+struct NoHook {
+    HD void operator()() const {}
+};
+
+template <int N1, int N2, class Sync, class Store, class Hook = NoHook>
 HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
                        const int* neg, const int* half, const Centre& centre, int tid, int nt,
-                       Sync sync, Store store)
+                       Sync sync, Store store, Hook cols_done = Hook{})
 {
     constexpr int N = N1 * N2;
     // forward along rows (centring the tile on the way in): lanes take consecutive rows
@@ -560,6 +571,7 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
         inv_a_lim<N1, N2>(Z + half[c], RS, n2, tw, rows_out);
     }
     sync();
+    cols_done();
     const int np = (rows_out + 1) / 2;
     if (rows_out + np <= N) {
         // placement rows 2q and 2q + 1 as one row A + i B at tile row rows_out + q; positions off

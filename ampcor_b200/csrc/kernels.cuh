@@ -226,6 +226,13 @@ struct SpecGeom {
     // tile, right after the partial sums
     int nseg;
     int smem_bytes;
+    // staged form (spec_staged_kernel, windows copied in while the previous pair finishes): the
+    // window's W rows of stage_rs floats at off_stage (over the tile's last rows), the copy's
+    // mbarrier at off_bar (and the CTA's wait-failure flag right after it);
+    // tile rows below stage_y0 are written straight from the staged copy, the rows from stage_y0 on
+    // in groups of stage_pj x 16 rows read whole before they are written
+    int off_stage, off_bar, stage_y0, stage_pj, stage_rs;
+    int smem_staged;  // 0: no staged form for this stage
 };
 
 // float amplitude tiles of chunk-local pair b (global pair pair0 + b): at base + off[pair0 + b]
@@ -318,5 +325,10 @@ cudaError_t launch_spec_reduce(const SpecGeom& full, int K, unsigned blocks, cud
 cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, SpecSource src,
                         long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out);
+// the staged form: min(pairs, sms) resident CTAs walk the chunk; a bounded wait that runs out is
+// counted in errs
+cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
+                               long long pair0, long long pairs, const long long* valid, InvSource inv,
+                               const float2* tw, SpecOut out, unsigned int* errs);
 
 }  // namespace ampcor_b200

@@ -21,8 +21,11 @@
 // error of a normalised correlation near 1e-7; the plain form's FP32 direct sums land in the same
 // range.  Where a nearly flat box would magnify the transform error, the numerator is recomputed
 // as a direct sum (spec_surface).
+#include <algorithm>
+
 #include "fft.cuh"
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 #include "tile_common.cuh"
 
 namespace ampcor_b200 {
@@ -113,13 +116,15 @@ __device__ __forceinline__ const float* spec_win(const SpecSource& s, long long 
 constexpr float kSpecErr = 1e-6f;
 constexpr float kSpecTol = 1e-5f;
 
-// Scratch of the placement statistics while the chip waits in registers: slot k is the imaginary
-// part of tile sample k, and past the tile's nz samples it continues in the tail buffer.
+// Scratch of the placement statistics: slot k is z[st k] for k below nz (the imaginary parts of
+// the tile while the chip waits in registers, st = 2; or a free stretch of the tile, st = 1), and
+// past them it continues in the tail buffer.
 struct StatSlots {
-    float* z;  // imaginary part of tile sample 0 (slots 2 floats apart)
+    float* z;  // slot 0
     float* tail;
     int nz;
-    __device__ __forceinline__ float* at(int k) const { return k < nz ? z + 2 * k : tail + (k - nz); }
+    int st;    // slot stride (floats)
+    __device__ __forceinline__ float* at(int k) const { return k < nz ? z + st * k : tail + (k - nz); }
 };
 
 __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
@@ -128,9 +133,9 @@ __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
     return var > 0.0f ? __frsqrt_rn(var) : 0.0f;
 }
 
-// 1/sigma_box of every placement from the window in the tile's real parts (rows RS apart), the
-// values shifted by sx (the window mean: the box variance does not change and the column sums
-// keep their digits).  sigma^2 = S2 - S1^2 / R^2 over the R x R box, its sum of squared deviations
+// 1/sigma_box of every placement from the window (win(y, x): the tile's real parts, or a staged
+// copy of the window), the values shifted by sx (the window mean: the box variance does not
+// change and the column sums keep their digits).  sigma^2 = S2 - S1^2 / R^2 over the R x R box, its sum of squared deviations
 // from its mean: the target variance of correlate.cu:196-309, whose box mean comes from the
 // summed-area table (tgtStats.cu).
 //
@@ -140,18 +145,18 @@ __device__ __forceinline__ float box_inv_of(double b1, double b2, double rcells)
 // column sum); after one exchange (part, FP64) each thread starts its share at V(0) plus the
 // earlier shares' slides (as a float pair) and adds the FP32 sum of its own slides so far, and
 // writes V(u, x) of its rows as floats into the slots (V1 at slot u W + x, V2 at C W + u W + x).
-// Then one warp per placement row (two rows at a time) forms the box sums
+// Then one warp per placement row (three rows at a time) forms the box sums
 // S(v) = sum_{x in [v, v + R)} V(x): S(0) as an FP64 warp sum, the others as S(0) plus an FP32 scan
 // of V(v + R) - V(v) across the lanes.  The phases are bound by instruction issue, so the FP64
 // work and the float-double conversions are kept to a few per column.  Ends with a barrier.
-template <int RS, int NT>
-__device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, StatSlots vs, double* part,
+template <int NT, class Win>
+__device__ void spec_box_stats(Win win, const SpecGeom& g, float sx, StatSlots vs, double* part,
                                float* invs)
 {
     const int R = g.R, W = g.W, C = g.C, nseg = g.nseg, D = C - 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int x = tid % W, s = tid / W;
-    auto tv = [&](int y) { return Z[y * RS + x].x - sx; };
+    auto tv = [&](int y) { return win(y, x) - sx; };
     constexpr int kRun = 8;
     if (s < nseg) {
         double b1 = 0.0, b2 = 0.0;
@@ -169,11 +174,22 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
             b2 += (double)r2;
         }
         float e1 = 0.0f, e2 = 0.0f;
-        for (int i = s * D / nseg, i1 = (s + 1) * D / nseg; i < i1; ++i) {
-            const float a = Z[(i + R) * RS + x].x, b = Z[i * RS + x].x;
-            const float d = a - b;
-            e1 += d;
-            e2 = fmaf(d, (a + b) - 2.0f * sx, e2);
+        constexpr int kA = 4;  // window rows read ahead of the sums
+        for (int i0 = s * D / nseg, i1 = (s + 1) * D / nseg; i0 < i1; i0 += kA) {
+            float a[kA], b[kA];
+#pragma unroll
+            for (int k = 0; k < kA; ++k) {
+                const int i = min(i0 + k, i1 - 1);
+                a[k] = win(i + R, x);
+                b[k] = win(i, x);
+            }
+#pragma unroll
+            for (int k = 0; k < kA; ++k)
+                if (i0 + k < i1) {
+                    const float d = a[k] - b[k];
+                    e1 += d;
+                    e2 = fmaf(d, (a[k] + b[k]) - 2.0f * sx, e2);
+                }
         }
         part[(0 * nseg + s) * W + x] = b1;
         part[(1 * nseg + s) * W + x] = b2;
@@ -203,8 +219,8 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
 #pragma unroll
             for (int k = 0; k < kB; ++k) {
                 const int i = min(i0 + k, i1 - 1);
-                a[k] = Z[(i + R) * RS + x].x;
-                b[k] = Z[i * RS + x].x;
+                a[k] = win(i + R, x);
+                b[k] = win(i, x);
             }
 #pragma unroll
             for (int k = 0; k < kB; ++k)
@@ -223,13 +239,20 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
     }
     __syncthreads();
     const double rcells = 1.0 / ((double)R * (double)R);
-    for (int u = warp; u < C; u += 2 * (NT / 32)) {
-        // rows u and u + (NT / 32); the second is row C - 1 again (not stored) past the end
-        const int uu[2] = {u, min(u + (NT / 32), C - 1)};
-        const bool keep2 = u + (NT / 32) < C;
-        double s1[2], s2[2];
+    // KR placement rows per warp at a time, u0, u0 + NW, ...; rows past the end repeat row C - 1
+    // (not stored), so that every warp runs one pass for C <= KR NW
+    constexpr int NW = NT / 32, KR = 3;
+    for (int u0 = warp; u0 < C; u0 += KR * NW) {
+        int uu[KR];
+        bool keep[KR];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < KR; ++r) {
+            uu[r] = min(u0 + r * NW, C - 1);
+            keep[r] = u0 + r * NW < C;
+        }
+        double s1[KR], s2[KR];
+#pragma unroll
+        for (int r = 0; r < KR; ++r) {
             float f1 = 0.0f, f2 = 0.0f;
             for (int c = lane; c < R; c += 32) {
                 f1 += *vs.at(uu[r] * W + c);
@@ -241,19 +264,19 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
+            for (int r = 0; r < KR; ++r) {
                 s1[r] += __shfl_xor_sync(kFull, s1[r], o);
                 s2[r] += __shfl_xor_sync(kFull, s2[r], o);
             }
-        if (lane == 0) {
-            invs[uu[0] * C] = box_inv_of(s1[0], s2[0], rcells);
-            if (keep2) invs[uu[1] * C] = box_inv_of(s1[1], s2[1], rcells);
-        }
+        if (lane == 0)
+#pragma unroll
+            for (int r = 0; r < KR; ++r)
+                if (keep[r]) invs[uu[r] * C] = box_inv_of(s1[r], s2[r], rcells);
         for (int j0 = 0; j0 < D; j0 += 32) {
             const int j = j0 + lane;
-            float i1[2], i2[2];
+            float i1[KR], i2[KR];
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
+            for (int r = 0; r < KR; ++r) {
                 i1[r] = 0.0f;
                 i2[r] = 0.0f;
                 if (j < D) {
@@ -264,7 +287,7 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1)
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < KR; ++r) {
                     const float y1 = __shfl_up_sync(kFull, i1[r], o);
                     const float y2 = __shfl_up_sync(kFull, i2[r], o);
                     if (lane >= o) {
@@ -272,13 +295,13 @@ __device__ void spec_box_stats(const float2* Z, const SpecGeom& g, float sx, Sta
                         i2[r] += y2;
                     }
                 }
-            if (j < D) {
-                invs[uu[0] * C + j + 1] = box_inv_of(s1[0] + (double)i1[0], s2[0] + (double)i2[0], rcells);
-                if (keep2)
-                    invs[uu[1] * C + j + 1] = box_inv_of(s1[1] + (double)i1[1], s2[1] + (double)i2[1], rcells);
-            }
+            if (j < D)
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < KR; ++r)
+                    if (keep[r])
+                        invs[uu[r] * C + j + 1] = box_inv_of(s1[r] + (double)i1[r], s2[r] + (double)i2[r], rcells);
+#pragma unroll
+            for (int r = 0; r < KR; ++r) {
                 s1[r] += (double)__shfl_sync(kFull, i1[r], 31);
                 s2[r] += (double)__shfl_sync(kFull, i2[r], 31);
             }
@@ -342,6 +365,28 @@ __device__ void spec_surface(float* G, double* red, const SpecGeom& g, const flo
             if (out1) out1[idx] = gv;
             if (out2) out2[idx] = gv;
         }
+    }
+}
+
+// the stage's result of pair p from the first maximum bv at placement bi: the coarse cell and its
+// nudged refinement corners (stage 0), or the refined cell and peak (stage 1)
+__device__ void spec_result(const SpecOut& out, long long p, int R, int W, int C, float bv, int bi)
+{
+    const int u = bi / C, v = bi - u * C;
+    if (out.stage == 0) {
+        // nudge.cu:107-140 (argument roles from nudge.cu:57: old = W, new = R + 2m)
+        const int m = out.m;
+        const int E = R + 2 * m;
+        int left = v - m;
+        if (left < 0) left = 0;
+        if (left + E > W) left = W - E;
+        int top = u - m;
+        if (top < 0) top = 0;
+        if (top + E > W) top = W - E;
+        out.coarse[p] = CoarseOut{u, v, top, left};
+        out.coarse_peak[p] = bv;
+    } else {
+        out.fine[p] = FineOut{u, v, bv, 0.0f};
     }
 }
 
@@ -476,8 +521,9 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
     if (!inv_b) {
         double* part = reinterpret_cast<double*>(ssm + g.off_gam);
-        const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS};
-        spec_box_stats<RS, kSpecThreads>(Z, g, centre.sx, vs, part, invs);
+        const StatSlots vs{Zf + 1, reinterpret_cast<float*>(part + 4 * g.nseg * W), N * RS, 2};
+        spec_box_stats<kSpecThreads>([&](int y, int x) { return Z[y * RS + x].x; }, g, centre.sx, vs,
+                                     part, invs);
     }
     // the zero-mean chip into the imaginary parts, zeros around it
 #pragma unroll
@@ -513,23 +559,337 @@ spec_kernel(SpecSource src, long long pair0, long long pairs, const long long* v
     float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
     float* gam = out.stage == 1 ? out.gam + (long long)blockIdx.x * C * C : nullptr;
     spec_surface<kSpecThreads>(G, red, g, invs, inv_sigma, mean_c, ebox, chip, cs, win, ws, gam, surf, bv, bi, flagged);
+    if (tid == 0) spec_result(out, p, R, W, C, bv, bi);
+}
+
+// ------------------------------------------------------------------------------------------
+// staged spectral correlation: one resident CTA per SM walks the pairs of a chunk
+// ------------------------------------------------------------------------------------------
+//
+// spec_kernel holds one CTA per SM (its tile fills the shared memory), so nothing hides the wait
+// for its tiles or the two sweeps of block sums that precede the transform; clock stamps put them
+// at a third of the fine stage.  Here a CTA stays resident and walks pairs blockIdx.x,
+// blockIdx.x + gridDim.x, ...: once a pair's inverse column pass is done (from then on its
+// correlation touches only the tile's first rows) the bulk-copy engine brings the next pair's
+// window (W x W dense floats, one cp.async.bulk completing on an mbarrier) into the tile's last
+// bytes, and the chip's bytes are sent toward L2.  A pair then starts with its window in shared
+// memory: the window's sums and placement statistics read from the staged copy (the tile's first
+// bytes are the statistics' scratch), then one pass that writes the window and the chip (loaded
+// from L2 meanwhile) into the tile and takes the chip's FP64 sums; the first transform pass takes
+// both means off.  The numerics are spec_kernel's.  Every wait is bounded; one that
+// runs out is counted in errs, the CTA lets the copy in flight land (again bounded) and returns.
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bytes (a multiple of 16) from global src to shared dst, both 16-byte aligned; completes on bar
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// RASTER false: the refined tiles, every pair's window W x W dense floats on a 16-byte boundary
+// (one copy), its statistics formed here; RASTER true: windows cut from a raster (a copy per row
+// from the 16-byte boundary at or before its first sample, rows stage_rs floats apart in the
+// staging bytes), the statistics given
+template <int N1, int N2, bool RASTER>
+__global__ void __launch_bounds__(kSpecThreads, 1)
+spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
+                   InvSource inv, const float2* tw_g, SpecOut out, unsigned int* errs)
+{
+    extern __shared__ __align__(16) unsigned char ssm[];
+    constexpr int N = N1 * N2;
+    constexpr int RS = N + 1;
+    constexpr int JN = (N + kSpecWarps - 1) / kSpecWarps, IN = (N + 31) / 32;
+    constexpr int PJ = 3;  // row groups of a piece read whole before it is written
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int W = g.W, R = g.R, C = g.C, SW = g.stage_rs;
+    float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
+    float* Zf = reinterpret_cast<float*>(Z);
+    float2* tw = reinterpret_cast<float2*>(ssm + g.off_tw);
+    int* neg = reinterpret_cast<int*>(ssm + g.off_neg);
+    int* half = reinterpret_cast<int*>(ssm + g.off_half);
+    double* red = reinterpret_cast<double*>(ssm + g.off_red);
+    float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
+    float* G = reinterpret_cast<float*>(ssm + g.off_gam);
+    float* stage = reinterpret_cast<float*>(ssm + g.off_stage);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ssm + g.off_bar);
+    int& s_err = *reinterpret_cast<int*>(ssm + g.off_bar + 8);  // a wait ran out (CTA-wide)
+    const long long cs = src.chip_stride, ws = src.win_stride;
+    const int jA = g.stage_y0 / kSpecWarps;
+    // a row's first sample sits xo floats past a 16-byte boundary; the row is copied from that
+    // boundary in whole 16-byte units, to stage + y SW
+    auto xo_of = [](const float* q) { return (int)((reinterpret_cast<uintptr_t>(q) >> 2) & 3); };
+
+    for (int k = tid; k < N; k += kSpecThreads) {
+        tw[k] = __ldg(tw_g + k);
+        neg[k] = fft::neg_pos<N1, N2>(k);
+    }
+    if (warp == 0) build_half<N1, N2>(half);
     if (tid == 0) {
-        const int u = bi / C, v = bi - u * C;
-        if (out.stage == 0) {
-            // nudge.cu:107-140 (argument roles from nudge.cu:57: old = W, new = R + 2m)
-            const int m = out.m;
-            const int E = R + 2 * m;
-            int left = v - m;
-            if (left < 0) left = 0;
-            if (left + E > W) left = W - E;
-            int top = u - m;
-            if (top < 0) top = 0;
-            if (top + E > W) top = W - E;
-            out.coarse[p] = CoarseOut{u, v, top, left};
-            out.coarse_peak[p] = bv;
-        } else {
-            out.fine[p] = FineOut{u, v, bv, 0.0f};
+        s_err = 0;
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // warp 0: the window rows of chunk pair b into the staging bytes, the chip rows toward L2; a
+    // pair without tiles (its offsets are -1) copies nothing and completes the phase at once
+    auto issue = [&](long long b) {
+        if (valid[pair0 + b] < 0) {
+            if (lane == 0) mbar_arrive(bar);
+            return;
         }
+        const float* w = spec_win(src, pair0, b);
+        const float* c = spec_chip(src, pair0, b);
+        if constexpr (!RASTER) {
+            if (lane == 0) {
+                const unsigned bytes = (unsigned)W * (unsigned)W * 4u;
+                mbar_expect_tx(bar, bytes);
+                bulk_to_smem(stage, w, bytes, bar);
+                bulk_prefetch_l2(c, (unsigned)R * (unsigned)cs * 4u);
+            }
+        } else {
+            unsigned bytes = 0;
+            for (int y = lane; y < W; y += 32) bytes += (unsigned)((xo_of(w + y * ws) + W + 3) & ~3) * 4u;
+            bytes = __reduce_add_sync(kFull, bytes);
+            if (lane == 0) mbar_expect_tx(bar, bytes);
+            __syncwarp();
+            for (int y = lane; y < W; y += 32) {
+                const float* q = w + y * ws;
+                const int xo = xo_of(q);
+                bulk_to_smem(stage + y * SW, q - xo, (unsigned)((xo + W + 3) & ~3) * 4u, bar);
+            }
+            for (int y = lane; y < R; y += 32) {
+                const float* q = c + y * cs;
+                const int xo = xo_of(q);
+                bulk_prefetch_l2(q - xo, (unsigned)((xo + R + 3) & ~3) * 4u);
+            }
+        }
+    };
+    if (warp == 0 && blockIdx.x < pairs) issue(blockIdx.x);
+    uint32_t parity = 0;
+    bool inflight = blockIdx.x < pairs;
+    for (long long b = blockIdx.x; b < pairs; b += gridDim.x) {
+        const long long p = pair0 + b;
+        const long long bn = b + gridDim.x;
+        const bool ok = valid[p] >= 0;
+        const float* chip = spec_chip(src, pair0, b);
+        const float* win = spec_win(src, pair0, b);
+        const float* inv_b = !RASTER ? nullptr : inv.off ? inv.base + inv.off[p] : inv.base + b * C * C;
+        const long long is = inv.off ? inv.stride : C;
+        const bool landed = mbar_wait(bar, parity, &s_err);
+        if (__syncthreads_or(!landed)) break;
+        parity ^= 1u;
+        inflight = false;
+        if (!ok) {
+            if (out.stage == 0 && tid == 0) {
+                out.coarse[p] = CoarseOut{-1, -1, -1, -1};
+                out.coarse_peak[p] = NAN;
+            }
+            if (bn < pairs) {
+                fence_async_smem();
+                __syncthreads();
+                if (warp == 0) issue(bn);
+                inflight = true;
+            }
+            continue;
+        }
+        // given placement statistics come in by asynchronous copies, waited for before the last
+        // transform step
+        if constexpr (RASTER)
+            for (int u = warp; u < C; u += kSpecWarps)
+                for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
+        // window sample (y, x) in the staging bytes
+        const long long a0 = (long long)(reinterpret_cast<uintptr_t>(win) >> 2);
+        auto wat = [&](int y, int x) {
+            if constexpr (RASTER)
+                return stage[y * SW + (int)((a0 + y * ws) & 3) + x];
+            else
+                return stage[y * W + x];
+        };
+
+        // the window's sums of t - k and (t - k)^2 about a pivot k (its first sample), as
+        // spec_kernel takes them (in another order)
+        const float pk = wat(0, 0);
+        double wsum[2];
+        {
+            float sw = 0.0f, sw2 = 0.0f;
+            if constexpr (!RASTER) {
+                // four samples a load
+                const float4* s4 = reinterpret_cast<const float4*>(stage);
+                const int n4 = (W * W) >> 2;
+#pragma unroll 4
+                for (int k = tid; k < n4; k += kSpecThreads) {
+                    const float4 v = s4[k];
+                    const float t[4] = {v.x - pk, v.y - pk, v.z - pk, v.w - pk};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        sw += t[q];
+                        sw2 = fmaf(t[q], t[q], sw2);
+                    }
+                }
+            } else {
+                for (int y = warp; y < W; y += kSpecWarps) {
+                    const float* row = stage + y * SW + (int)((a0 + y * ws) & 3);
+#pragma unroll 4
+                    for (int x = lane; x < W; x += 32) {
+                        const float t = row[x] - pk;
+                        sw += t;
+                        sw2 = fmaf(t, t, sw2);
+                    }
+                }
+            }
+            wsum[0] = sw;
+            wsum[1] = sw2;
+            block_sum2<kSpecWarps>(wsum[0], wsum[1], red);
+        }
+        const double cells_c = (double)R * (double)R, cells_w = (double)W * (double)W;
+        const double mean_w = (double)pk + wsum[0] / cells_w;
+        const double st = fmax(wsum[1] - wsum[0] * wsum[0] / cells_w, 0.0) + 1e-5 * wsum[1];
+        const float sx = (float)mean_w;
+
+        // placement statistics from the staged window where none are given; their scratch is the
+        // tile's first bytes
+        if constexpr (!RASTER) {
+            double* part = reinterpret_cast<double*>(ssm + g.off_gam);
+            const StatSlots vs{Zf, reinterpret_cast<float*>(part + 4 * g.nseg * W), g.off_stage / 4, 1};
+            spec_box_stats<kSpecThreads>(wat, g, sx, vs, part, invs);
+        }
+
+        // window (real parts) and chip (imaginary parts; its bytes were sent toward L2 with the
+        // window) into the tile, zeros around them; the chip's FP64 sum and sum of squares as it
+        // goes (every product of two floats is exact in FP64), per warp
+        float cr[JN][IN];
+#pragma unroll
+        for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int i = 0; i < IN; ++i) {
+                const int y = warp + kSpecWarps * j, x = lane + 32 * i;
+                cr[j][i] = y < R && x < R ? __ldg(chip + y * cs + x) : 0.0f;
+            }
+        double c1 = 0.0, c2 = 0.0;
+        auto put = [&](int j, int i, float t) {
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
+            if (y < N && x < N) {
+                const float c = cr[j][i];
+                c1 += (double)c;
+                c2 = fma((double)c, (double)c, c2);
+                Z[y * RS + x] = make_float2(t, c);
+            }
+        };
+        auto staged = [&](int j, int i) {
+            const int y = warp + kSpecWarps * j, x = lane + 32 * i;
+            return y < W && x < W ? wat(y, x) : 0.0f;
+        };
+        // rows below stage_y0 lie below the staged bytes: written as they are read
+#pragma unroll
+        for (int j = 0; j < JN; ++j)
+            if (j < jA)
+#pragma unroll
+                for (int i = 0; i < IN; ++i) put(j, i, staged(j, i));
+        __syncthreads();
+        // the others cover staged bytes: each piece is read whole, then written (a piece's rows
+        // never reach the staged rows of a later piece)
+#pragma unroll
+        for (int j0 = 0; j0 < JN; j0 += PJ) {
+            if (j0 + PJ <= jA) continue;
+            float v[PJ][IN];
+#pragma unroll
+            for (int q = 0; q < PJ; ++q)
+#pragma unroll
+                for (int i = 0; i < IN; ++i) v[q][i] = j0 + q < JN && j0 + q >= jA ? staged(j0 + q, i) : 0.0f;
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < PJ; ++q)
+                if (j0 + q < JN && j0 + q >= jA)
+#pragma unroll
+                    for (int i = 0; i < IN; ++i) put(j0 + q, i, v[q][i]);
+        }
+        c1 = warp_sum(c1);
+        c2 = warp_sum(c2);
+        if (lane == 0) {
+            red[2 * warp] = c1;
+            red[2 * warp + 1] = c2;
+        }
+        __syncthreads();
+        double s1 = 0.0, s2 = 0.0;
+        for (int w = 0; w < kSpecWarps; ++w) {
+            s1 += red[2 * w];
+            s2 += red[2 * w + 1];
+        }
+        // |r'|^2 = S2 - S1^2 / R^2 of the zero-mean chip; a chip flat to within its own rounding
+        // (a constant: its zero-mean values are exactly 0) gets 0, as spec_kernel's sum of the
+        // squared zero-mean values gives it
+        const double mean_c = s1 / cells_c;
+        const double ss = s2 - s1 * mean_c;
+        const float inv_sigma = ss > 1e-14 * s2 ? (float)(1.0 / sqrt(ss)) : 0.0f;
+        const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
+        // the window mean and the chip's mean come off as the first transform pass reads the tile
+        fft::Centre centre{sx, W};
+        centre.ci_hi = mc_hi;
+        centre.ci_lo = mc_lo;
+        centre.ci = R;
+
+        const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
+        const float ebox = kSpecErr * (float)sqrt(st);
+        float bv = -INFINITY;
+        int bi = INT_MAX;
+        int flagged = 0;
+        fft::correlate_tile<N1, N2>(
+            Z, RS, W, C, tw, neg, half, centre, tid, kSpecThreads, BlockSync{},
+            [&](int u, int v, float2 val) {
+                if (v < C) {
+                    const int idx = u * C + v;
+                    const float inv_box = invs[idx];
+                    const float gv = val.x * scale * inv_box * inv_sigma;
+                    G[idx] = gv;
+                    if (ebox * inv_box > kSpecTol)
+                        flagged = 1;
+                    else
+                        better(bv, bi, gv, idx);
+                }
+            },
+            [&]() {
+                // the given statistics have landed; the staged bytes are free from here on: the
+                // next pair's window comes in
+                if constexpr (RASTER) cp_async_wait_all();
+                fence_async_smem();
+                __syncthreads();
+                if (bn < pairs) {
+                    if (warp == 0) issue(bn);
+                    inflight = true;
+                }
+            });
+
+        float* surf = out.surfaces ? out.surfaces + (size_t)p * C * C : nullptr;
+        float* gam = out.stage == 1 ? out.gam + b * C * C : nullptr;
+        spec_surface<kSpecThreads>(G, red, g, invs, inv_sigma, mean_c, ebox, chip, cs, win, ws, gam, surf, bv, bi,
+                                   flagged);
+        if (tid == 0) spec_result(out, p, R, W, C, bv, bi);
+    }
+    if (s_err) {
+        // a wait ran out: count it once per CTA and let the copy in flight land before the shared
+        // memory is given up
+        if (tid == 0) {
+            atomicAdd(errs, 1u);
+            if (inflight) {
+                const long long t0 = clock64();
+                while (!mbar_try(bar, parity) && clock64() - t0 < kSpinCycles) {
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1338,6 +1698,10 @@ cudaError_t spec_set_smem_limits()
     if (e == cudaSuccess)          \
         e = cudaFuncSetAttribute(spec_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
     if (e == cudaSuccess)          \
+        e = cudaFuncSetAttribute(spec_staged_kernel<A, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess)          \
+        e = cudaFuncSetAttribute(spec_staged_kernel<A, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess)          \
         e = cudaFuncSetAttribute(spec_block_kernel<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
 #undef AMPCOR_SPEC_CASE
@@ -1426,6 +1790,27 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
         spec_kernel<A, B><<<blocks, kSpecThreads, g.smem_bytes, st>>>(src, pair0, pairs, valid, g,  \
                                                                   inv, tw, out);                 \
         return cudaGetLastError();                                                               \
+    }
+    AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
+#undef AMPCOR_SPEC_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
+                               long long pair0, long long pairs, const long long* valid, InvSource inv,
+                               const float2* tw, SpecOut out, unsigned int* errs)
+{
+    if (pairs <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)std::min<long long>(pairs, std::max(1u, sms));
+#define AMPCOR_SPEC_CASE(NN, A, B)                                                                      \
+    if (g.N == NN) {                                                                                    \
+        if (inv.base)                                                                                   \
+            spec_staged_kernel<A, B, true><<<blocks, kSpecThreads, g.smem_staged, st>>>(src, pair0, pairs, valid, \
+                                                                                  g, inv, tw, out, errs); \
+        else                                                                                            \
+            spec_staged_kernel<A, B, false><<<blocks, kSpecThreads, g.smem_staged, st>>>(src, pair0, pairs,     \
+                                                                                   valid, g, inv, tw, out, errs); \
+        return cudaGetLastError();                                                                      \
     }
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
 #undef AMPCOR_SPEC_CASE
