@@ -9,6 +9,7 @@
 #include "../../include/ampcor_b200.h"
 #include "kernels.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -277,7 +278,7 @@ bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
     const long stage = (long)W * g.stage_rs * 4;
     const int np = (C + 1) / 2;
     const long kept = (long)(C + np <= N ? C + np : C) * row;
-    const long S = up(std::max(kept, tile - stage), 16);
+    const long S = up(std::max(kept, tile - stage), 128);
     if (2L * C * W * 4 > S) return false;
     const int y0 = (int)std::min<long>(N, S / row) / kSpecWarps * kSpecWarps;
     const int JN = (N + kSpecWarps - 1) / kSpecWarps;
@@ -901,6 +902,43 @@ struct SpecRasters {
 };
 
 // buffers of a spectral job of `pairs` pairs; no launches
+// cuTensorMapEncodeTiled from the driver (the runtime is linked statically; the driver's entry
+// point is looked up once)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<EncodeTiledFn>(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// a 2-D map of a float raster (lines x samples) whose boxes are bx x by floats (bx a multiple of
+// 4); false where the driver has no tensor maps or the raster breaks the copy engine's alignment
+// rules (a 16-byte aligned base, lines a multiple of 16 bytes)
+bool raster_map(CUtensorMap& m, const float* base, long long lines, long long samples, int bx, int by)
+{
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || (samples & 3) || lines < 1 || bx % 4 || bx < 4 ||
+        bx > 256 || by < 1 || by > 256)
+        return false;
+    const cuuint64_t dim[2] = {(cuuint64_t)samples, (cuuint64_t)lines};
+    const cuuint64_t stride[1] = {(cuuint64_t)samples * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+    const cuuint32_t es[2] = {1, 1};
+    return fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dim, stride, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int spec_rasters(ampcor_handle* h, const PairSource& src, long long pairs, SpecRasters& r)
 {
     int rc = ensure_refined(h);
@@ -909,9 +947,12 @@ int spec_rasters(ampcor_handle* h, const PairSource& src, long long pairs, SpecR
     r.shared = src.ref_base == src.tgt_base;
     const size_t need = (size_t)src.ref_count + (r.shared ? 0 : (size_t)src.tgt_count);
     // 16 floats of slack here and below: staged copies round rows out to 16-byte boundaries
-    if ((rc = grow(h, h->d_amp, h->amp_cap, need + 16, "amplitude rasters"))) return rc;
+    // the secondary's amplitudes start on a 16-byte boundary (tensor copies of its windows)
+    const size_t ref_span = ((size_t)src.ref_count + 3) & ~(size_t)3;
+    const size_t need_al = r.shared ? need : ref_span + (size_t)src.tgt_count;
+    if ((rc = grow(h, h->d_amp, h->amp_cap, need_al + 16, "amplitude rasters"))) return rc;
     r.amp_ref = h->d_amp;
-    r.amp_tgt = r.shared ? h->d_amp : h->d_amp + src.ref_count;
+    r.amp_tgt = r.shared ? h->d_amp : h->d_amp + ref_span;
     // coarse box statistics once per raster where the windows tile a raster (they overlap), else
     // inside the correlation kernel from the window it holds (as for every fine window)
     r.rows = src.tgt_lines - h->R + 1;
@@ -973,6 +1014,13 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
     const SpecSource cs{r.amp_ref, src.ref_stride, src.ref_off, 0, r.amp_tgt, src.tgt_stride, src.tgt_off, 0};
     const SpecSource fs{h->d_refined, h->Rf, nullptr, h->refined_stride,
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
+    // the staged coarse stage takes its windows from the secondary's amplitude raster through a
+    // tensor map and its statistics from the raster
+    CUtensorMap wmap{}, cmap{};
+    const bool coarse_st =
+        h->coarse_staged && r.inv_c.base && src.tgt_stride > 0 && src.ref_stride > 0 &&
+        raster_map(wmap, r.amp_tgt, src.tgt_count / src.tgt_stride, src.tgt_stride, h->spc_st.stage_rs, h->W) &&
+        raster_map(cmap, r.amp_ref, src.ref_count / src.ref_stride, src.ref_stride, (h->R + 6) & ~3, h->R);
     for (long long c0 = p0; c0 < p1; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, p1 - c0);
         cudaEvent_t b = mark(h, st);
@@ -998,10 +1046,10 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                                      h->d_part, h->d_scal, co),
                "launching the coarse reduction");
         } else {
-            // the staged form of the coarse stage takes its statistics from the raster
-            if (h->coarse_staged && r.inv_c.base)
+            if (coarse_st)
                 CK(h, launch_spec_staged(h->spc_st, (unsigned)h->sms, st, cs, c0, n, src.ref_off, r.inv_c,
-                                         reinterpret_cast<const float2*>(h->d_tw_c), co, h->d_tc_err),
+                                         reinterpret_cast<const float2*>(h->d_tw_c), co, h->d_tc_err,
+                                         &wmap, &cmap),
                    "launching the staged coarse correlation");
             else
                 CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
@@ -1048,7 +1096,8 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
             if (h->fine_staged)
                 CK(h, launch_spec_staged(h->spf_st, (unsigned)h->sms, st, fs, c0, n, src.ref_off,
                                          InvSource{nullptr, nullptr, 0},
-                                         reinterpret_cast<const float2*>(h->d_tw_f), fo, h->d_tc_err),
+                                         reinterpret_cast<const float2*>(h->d_tw_f), fo, h->d_tc_err,
+                                         nullptr, nullptr),
                    "launching the staged fine correlation");
             else
                 CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},
@@ -1181,9 +1230,7 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         // pair are dense rows of one buffer, staged whole when its rows are 16-byte multiples
         const char* stg = std::getenv("AMPCOR_STAGED");
         const bool staged_on = !(stg && std::strcmp(stg, "0") == 0);
-        // (the coarse stage stays on spec_kernel: a bulk copy per window row takes longer to issue
-        // than the tail of the previous pair)
-        h->coarse_staged = false;
+        h->coarse_staged = staged_on && direct_c && plan_spec_staged(h->R, h->W, false, h->spc_st);
         h->fine_staged = staged_on && direct_f &&
                          plan_spec_staged(h->Rf, h->Wf, h->Rf % 2 == 0 && h->Wf % 2 == 0, h->spf_st) &&
                          h->spf_st.stage_rs == h->Wf;

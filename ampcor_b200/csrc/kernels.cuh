@@ -14,6 +14,7 @@
 //                    (offsets.cu:86-129).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -326,9 +327,12 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
                         long long pair0, long long pairs, const long long* valid, InvSource inv,
                         const float2* tw, SpecOut out);
 // the staged form: min(pairs, sms) resident CTAs walk the chunk; a bounded wait that runs out is
-// counted in errs
+// counted in errs.  Refined tiles: wmap and cmap null, no statistics given.  Raster windows:
+// wmap and cmap 2-D maps of the secondary and reference amplitude rasters with boxes of
+// stage_rs x W and (R + 6 & ~3) x R floats, the statistics given (inv).
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
-                               const float2* tw, SpecOut out, unsigned int* errs);
+                               const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
+                               const CUtensorMap* cmap);
 
 }  // namespace ampcor_b200

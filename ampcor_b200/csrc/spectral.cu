@@ -23,6 +23,8 @@
 // as a direct sum (spec_surface).
 #include <algorithm>
 
+#include <cuda.h>
+
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "tcgen05.cuh"
@@ -599,14 +601,32 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
+// the box of a 2-D tensor map at (x, y) (x a multiple of 4 floats) into shared dst; completes on bar
+__device__ __forceinline__ void tensor_to_smem(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            saddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tensor_prefetch_l2(const CUtensorMap* map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
+}
+
 // RASTER false: the refined tiles, every pair's window W x W dense floats on a 16-byte boundary
-// (one copy), its statistics formed here; RASTER true: windows cut from a raster (a copy per row
-// from the 16-byte boundary at or before its first sample, rows stage_rs floats apart in the
-// staging bytes), the statistics given
+// (one copy), its statistics formed here; RASTER true: windows cut from a raster, copied as the
+// box of wmap (stage_rs x W floats) whose first column is the 16-byte boundary at or before the
+// window's first sample, the chip's box of cmap sent toward L2, the statistics given
 template <int N1, int N2, bool RASTER>
 __global__ void __launch_bounds__(kSpecThreads, 1)
 spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
-                   InvSource inv, const float2* tw_g, SpecOut out, unsigned int* errs)
+                   InvSource inv, const float2* tw_g, SpecOut out, unsigned int* errs,
+                   const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap cmap)
 {
     extern __shared__ __align__(16) unsigned char ssm[];
     constexpr int N = N1 * N2;
@@ -628,9 +648,6 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
     int& s_err = *reinterpret_cast<int*>(ssm + g.off_bar + 8);  // a wait ran out (CTA-wide)
     const long long cs = src.chip_stride, ws = src.win_stride;
     const int jA = g.stage_y0 / kSpecWarps;
-    // a row's first sample sits xo floats past a 16-byte boundary; the row is copied from that
-    // boundary in whole 16-byte units, to stage + y SW
-    auto xo_of = [](const float* q) { return (int)((reinterpret_cast<uintptr_t>(q) >> 2) & 3); };
 
     for (int k = tid; k < N; k += kSpecThreads) {
         tw[k] = __ldg(tw_g + k);
@@ -660,20 +677,13 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
                 bulk_prefetch_l2(c, (unsigned)R * (unsigned)cs * 4u);
             }
         } else {
-            unsigned bytes = 0;
-            for (int y = lane; y < W; y += 32) bytes += (unsigned)((xo_of(w + y * ws) + W + 3) & ~3) * 4u;
-            bytes = __reduce_add_sync(kFull, bytes);
-            if (lane == 0) mbar_expect_tx(bar, bytes);
-            __syncwarp();
-            for (int y = lane; y < W; y += 32) {
-                const float* q = w + y * ws;
-                const int xo = xo_of(q);
-                bulk_to_smem(stage + y * SW, q - xo, (unsigned)((xo + W + 3) & ~3) * 4u, bar);
-            }
-            for (int y = lane; y < R; y += 32) {
-                const float* q = c + y * cs;
-                const int xo = xo_of(q);
-                bulk_prefetch_l2(q - xo, (unsigned)((xo + R + 3) & ~3) * 4u);
+            if (lane == 0) {
+                const long long wo = src.win_off[pair0 + b], co = src.chip_off[pair0 + b];
+                const int wy = (int)(wo / ws), wx = (int)(wo - (long long)wy * ws);
+                const int cy = (int)(co / cs), cx = (int)(co - (long long)cy * cs);
+                mbar_expect_tx(bar, (unsigned)W * (unsigned)SW * 4u);
+                tensor_to_smem(stage, &wmap, wx & ~3, wy, bar);
+                tensor_prefetch_l2(&cmap, cx & ~3, cy);
             }
         }
     };
@@ -710,11 +720,11 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         if constexpr (RASTER)
             for (int u = warp; u < C; u += kSpecWarps)
                 for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
-        // window sample (y, x) in the staging bytes
-        const long long a0 = (long long)(reinterpret_cast<uintptr_t>(win) >> 2);
+        // window sample (y, x) in the staging bytes: the box starts xo samples before the window
+        const int xo = RASTER ? (int)((src.win_off[p] % ws) & 3) : 0;
         auto wat = [&](int y, int x) {
             if constexpr (RASTER)
-                return stage[y * SW + (int)((a0 + y * ws) & 3) + x];
+                return stage[y * SW + xo + x];
             else
                 return stage[y * W + x];
         };
@@ -740,11 +750,17 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
                     }
                 }
             } else {
-                for (int y = warp; y < W; y += kSpecWarps) {
-                    const float* row = stage + y * SW + (int)((a0 + y * ws) & 3);
+                // four box samples a load, those outside the window's columns left out
+                const float4* s4 = reinterpret_cast<const float4*>(stage);
+                const int q4 = SW >> 2, n4 = W * q4;
 #pragma unroll 4
-                    for (int x = lane; x < W; x += 32) {
-                        const float t = row[x] - pk;
+                for (int k = tid; k < n4; k += kSpecThreads) {
+                    const float4 v = s4[k];
+                    const int c0 = 4 * (k % q4) - xo;
+                    const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float t = c0 + q >= 0 && c0 + q < W ? e[q] - pk : 0.0f;
                         sw += t;
                         sw2 = fmaf(t, t, sw2);
                     }
@@ -1798,18 +1814,19 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
-                               const float2* tw, SpecOut out, unsigned int* errs)
+                               const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
+                               const CUtensorMap* cmap)
 {
     if (pairs <= 0) return cudaSuccess;
     const unsigned blocks = (unsigned)std::min<long long>(pairs, std::max(1u, sms));
 #define AMPCOR_SPEC_CASE(NN, A, B)                                                                      \
     if (g.N == NN) {                                                                                    \
-        if (inv.base)                                                                                   \
-            spec_staged_kernel<A, B, true><<<blocks, kSpecThreads, g.smem_staged, st>>>(src, pair0, pairs, valid, \
-                                                                                  g, inv, tw, out, errs); \
+        if (wmap)                                                                                       \
+            spec_staged_kernel<A, B, true><<<blocks, kSpecThreads, g.smem_staged, st>>>(                      \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, *wmap, *cmap);                             \
         else                                                                                            \
-            spec_staged_kernel<A, B, false><<<blocks, kSpecThreads, g.smem_staged, st>>>(src, pair0, pairs,     \
-                                                                                   valid, g, inv, tw, out, errs); \
+            spec_staged_kernel<A, B, false><<<blocks, kSpecThreads, g.smem_staged, st>>>(                     \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, CUtensorMap{}, CUtensorMap{});             \
         return cudaGetLastError();                                                                      \
     }
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
