@@ -298,14 +298,18 @@ bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
     g.off_half = (int)off;
     off = up(off + (long)(N / 2 + 1) * 4, 16);
     g.off_red = (int)off;
-    off += 2L * kSpecWarps * 8;
+    off += 4L * kSpecWarps * 8;
     g.off_inv = (int)off;
     off = up(off + (long)C * C * 4, 16);
     g.off_gam = (int)off;  // the surface; before the last step, the statistics' partial sums
     const long limit = 227L * 1024 - 16;
     g.nseg = std::max(1, kSpecThreads / W);
     while (g.nseg > 1 && off + 32L * g.nseg * W > limit) --g.nseg;
-    off = up(off + std::max<long>((long)C * C * 4, 32L * g.nseg * W), 16);
+    off = up(off + std::max<long>((long)C * C * 4, 32L * g.nseg * W), 128);
+    // raster statistics as the copy engine brings them (rows from the window's 16-byte boundary)
+    g.inv_rs = (C + 6) & ~3;
+    g.off_inv_raw = dense ? 0 : (int)off;
+    if (!dense) off = up(off + (long)C * g.inv_rs * 4, 16);
     g.off_bar = (int)off;
     off += 16;
     g.smem_staged = off <= limit + 16 ? (int)off : 0;
@@ -1016,11 +1020,12 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                         h->d_refined + (long long)h->Rf * h->Rf, h->Wf, nullptr, h->refined_stride};
     // the staged coarse stage takes its windows from the secondary's amplitude raster through a
     // tensor map and its statistics from the raster
-    CUtensorMap wmap{}, cmap{};
+    CUtensorMap wmap{}, cmap{}, imap{};
     const bool coarse_st =
         h->coarse_staged && r.inv_c.base && src.tgt_stride > 0 && src.ref_stride > 0 &&
         raster_map(wmap, r.amp_tgt, src.tgt_count / src.tgt_stride, src.tgt_stride, h->spc_st.stage_rs, h->W) &&
-        raster_map(cmap, r.amp_ref, src.ref_count / src.ref_stride, src.ref_stride, (h->R + 6) & ~3, h->R);
+        raster_map(cmap, r.amp_ref, src.ref_count / src.ref_stride, src.ref_stride, (h->R + 6) & ~3, h->R) &&
+        raster_map(imap, r.inv_c.base, r.rows, src.tgt_stride, h->spc_st.inv_rs, h->C);
     for (long long c0 = p0; c0 < p1; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, p1 - c0);
         cudaEvent_t b = mark(h, st);
@@ -1049,7 +1054,7 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
             if (coarse_st)
                 CK(h, launch_spec_staged(h->spc_st, (unsigned)h->sms, st, cs, c0, n, src.ref_off, r.inv_c,
                                          reinterpret_cast<const float2*>(h->d_tw_c), co, h->d_tc_err,
-                                         &wmap, &cmap),
+                                         &wmap, &cmap, &imap),
                    "launching the staged coarse correlation");
             else
                 CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
@@ -1097,7 +1102,7 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                 CK(h, launch_spec_staged(h->spf_st, (unsigned)h->sms, st, fs, c0, n, src.ref_off,
                                          InvSource{nullptr, nullptr, 0},
                                          reinterpret_cast<const float2*>(h->d_tw_f), fo, h->d_tc_err,
-                                         nullptr, nullptr),
+                                         nullptr, nullptr, nullptr),
                    "launching the staged fine correlation");
             else
                 CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},

@@ -233,6 +233,7 @@ struct SpecGeom {
     // tile rows below stage_y0 are written straight from the staged copy, the rows from stage_y0 on
     // in groups of stage_pj x 16 rows read whole before they are written
     int off_stage, off_bar, stage_y0, stage_pj, stage_rs;
+    int off_inv_raw, inv_rs;  // raster statistics as copied: C rows of inv_rs floats
     int smem_staged;  // 0: no staged form for this stage
 };
 
@@ -328,11 +329,12 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
                         const float2* tw, SpecOut out);
 // the staged form: min(pairs, sms) resident CTAs walk the chunk; a bounded wait that runs out is
 // counted in errs.  Refined tiles: wmap and cmap null, no statistics given.  Raster windows:
-// wmap and cmap 2-D maps of the secondary and reference amplitude rasters with boxes of
-// stage_rs x W and (R + 6 & ~3) x R floats, the statistics given (inv).
+// wmap, cmap and imap 2-D maps of the secondary and reference amplitude rasters and of the
+// secondary's box statistics (inv) with boxes of stage_rs x W, (R + 6 & ~3) x R and inv_rs x C
+// floats.
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
                                const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
-                               const CUtensorMap* cmap);
+                               const CUtensorMap* cmap, const CUtensorMap* imap);
 
 }  // namespace ampcor_b200

@@ -621,12 +621,14 @@ __device__ __forceinline__ void tensor_prefetch_l2(const CUtensorMap* map, int x
 // RASTER false: the refined tiles, every pair's window W x W dense floats on a 16-byte boundary
 // (one copy), its statistics formed here; RASTER true: windows cut from a raster, copied as the
 // box of wmap (stage_rs x W floats) whose first column is the 16-byte boundary at or before the
-// window's first sample, the chip's box of cmap sent toward L2, the statistics given
+// window's first sample, with the box of the raster's statistics (imap, inv_rs x C floats) at the
+// same corner, the chip's box of cmap sent toward L2
 template <int N1, int N2, bool RASTER>
 __global__ void __launch_bounds__(kSpecThreads, 1)
 spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
                    InvSource inv, const float2* tw_g, SpecOut out, unsigned int* errs,
-                   const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap cmap)
+                   const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap cmap,
+                   const __grid_constant__ CUtensorMap imap)
 {
     extern __shared__ __align__(16) unsigned char ssm[];
     constexpr int N = N1 * N2;
@@ -644,6 +646,7 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
     float* invs = reinterpret_cast<float*>(ssm + g.off_inv);
     float* G = reinterpret_cast<float*>(ssm + g.off_gam);
     float* stage = reinterpret_cast<float*>(ssm + g.off_stage);
+    float* inv_raw = reinterpret_cast<float*>(ssm + g.off_inv_raw);
     uint64_t* bar = reinterpret_cast<uint64_t*>(ssm + g.off_bar);
     int& s_err = *reinterpret_cast<int*>(ssm + g.off_bar + 8);  // a wait ran out (CTA-wide)
     const long long cs = src.chip_stride, ws = src.win_stride;
@@ -681,8 +684,9 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
                 const long long wo = src.win_off[pair0 + b], co = src.chip_off[pair0 + b];
                 const int wy = (int)(wo / ws), wx = (int)(wo - (long long)wy * ws);
                 const int cy = (int)(co / cs), cx = (int)(co - (long long)cy * cs);
-                mbar_expect_tx(bar, (unsigned)W * (unsigned)SW * 4u);
+                mbar_expect_tx(bar, ((unsigned)W * (unsigned)SW + (unsigned)C * (unsigned)g.inv_rs) * 4u);
                 tensor_to_smem(stage, &wmap, wx & ~3, wy, bar);
+                tensor_to_smem(inv_raw, &imap, wx & ~3, wy, bar);
                 tensor_prefetch_l2(&cmap, cx & ~3, cy);
             }
         }
@@ -696,8 +700,6 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         const bool ok = valid[p] >= 0;
         const float* chip = spec_chip(src, pair0, b);
         const float* win = spec_win(src, pair0, b);
-        const float* inv_b = !RASTER ? nullptr : inv.off ? inv.base + inv.off[p] : inv.base + b * C * C;
-        const long long is = inv.off ? inv.stride : C;
         const bool landed = mbar_wait(bar, parity, &s_err);
         if (__syncthreads_or(!landed)) break;
         parity ^= 1u;
@@ -715,13 +717,41 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
             }
             continue;
         }
-        // given placement statistics come in by asynchronous copies, waited for before the last
-        // transform step
-        if constexpr (RASTER)
-            for (int u = warp; u < C; u += kSpecWarps)
-                for (int v = lane; v < C; v += 32) cp_async4(invs + u * C + v, inv_b + u * is + v);
         // window sample (y, x) in the staging bytes: the box starts xo samples before the window
         const int xo = RASTER ? (int)((src.win_off[p] % ws) & 3) : 0;
+        // the chip to registers: for a raster window at once (its loads in flight while the
+        // statistics are moved and its sum taken before the tile is written), for the refined
+        // tiles after the statistics (registers are short there)
+        float cr[JN][IN];
+        auto load_chip = [&]() {
+#pragma unroll
+            for (int j = 0; j < JN; ++j)
+#pragma unroll
+                for (int i = 0; i < IN; ++i) {
+                    const int y = warp + kSpecWarps * j, x = lane + 32 * i;
+                    cr[j][i] = y < R && x < R ? __ldg(chip + y * cs + x) : 0.0f;
+                }
+        };
+        double mean_c = 0.0;
+        if constexpr (RASTER) {
+            load_chip();
+            // the raster's placement statistics, copied with the window, into their C x C layout
+            for (int u = warp; u < C; u += kSpecWarps)
+                for (int v = lane; v < C; v += 32) invs[u * C + v] = inv_raw[u * g.inv_rs + xo + v];
+            // the chip's FP64 mean (spec_kernel's first sweep)
+            double c1 = 0.0;
+#pragma unroll
+            for (int j = 0; j < JN; ++j)
+#pragma unroll
+                for (int i = 0; i < IN; ++i) c1 += (double)cr[j][i];
+            c1 = warp_sum(c1);
+            if (lane == 0) red[warp] = c1;
+            __syncthreads();
+            double t1 = 0.0;
+            for (int w = 0; w < kSpecWarps; ++w) t1 += red[w];
+            mean_c = t1 / ((double)R * (double)R);
+            __syncthreads();
+        }
         auto wat = [&](int y, int x) {
             if constexpr (RASTER)
                 return stage[y * SW + xo + x];
@@ -730,40 +760,23 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         };
 
         // the window's sums of t - k and (t - k)^2 about a pivot k (its first sample), as
-        // spec_kernel takes them (in another order)
+        // spec_kernel takes them (in another order): here for the refined window, whose
+        // statistics are centred on its mean; as the tile is written for a raster window
         const float pk = wat(0, 0);
-        double wsum[2];
-        {
+        double wsum[2] = {0.0, 0.0};
+        if constexpr (!RASTER) {
             float sw = 0.0f, sw2 = 0.0f;
-            if constexpr (!RASTER) {
-                // four samples a load
-                const float4* s4 = reinterpret_cast<const float4*>(stage);
-                const int n4 = (W * W) >> 2;
+            // four samples a load
+            const float4* s4 = reinterpret_cast<const float4*>(stage);
+            const int n4 = (W * W) >> 2;
 #pragma unroll 4
-                for (int k = tid; k < n4; k += kSpecThreads) {
-                    const float4 v = s4[k];
-                    const float t[4] = {v.x - pk, v.y - pk, v.z - pk, v.w - pk};
+            for (int k = tid; k < n4; k += kSpecThreads) {
+                const float4 v = s4[k];
+                const float t[4] = {v.x - pk, v.y - pk, v.z - pk, v.w - pk};
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        sw += t[q];
-                        sw2 = fmaf(t[q], t[q], sw2);
-                    }
-                }
-            } else {
-                // four box samples a load, those outside the window's columns left out
-                const float4* s4 = reinterpret_cast<const float4*>(stage);
-                const int q4 = SW >> 2, n4 = W * q4;
-#pragma unroll 4
-                for (int k = tid; k < n4; k += kSpecThreads) {
-                    const float4 v = s4[k];
-                    const int c0 = 4 * (k % q4) - xo;
-                    const float e[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float t = c0 + q >= 0 && c0 + q < W ? e[q] - pk : 0.0f;
-                        sw += t;
-                        sw2 = fmaf(t, t, sw2);
-                    }
+                for (int q = 0; q < 4; ++q) {
+                    sw += t[q];
+                    sw2 = fmaf(t[q], t[q], sw2);
                 }
             }
             wsum[0] = sw;
@@ -771,9 +784,9 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
             block_sum2<kSpecWarps>(wsum[0], wsum[1], red);
         }
         const double cells_c = (double)R * (double)R, cells_w = (double)W * (double)W;
-        const double mean_w = (double)pk + wsum[0] / cells_w;
-        const double st = fmax(wsum[1] - wsum[0] * wsum[0] / cells_w, 0.0) + 1e-5 * wsum[1];
-        const float sx = (float)mean_w;
+        double mean_w = (double)pk + wsum[0] / cells_w;
+        double st = fmax(wsum[1] - wsum[0] * wsum[0] / cells_w, 0.0) + 1e-5 * wsum[1];
+        float sx = (float)mean_w;
 
         // placement statistics from the staged window where none are given; their scratch is the
         // tile's first bytes
@@ -784,23 +797,33 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         }
 
         // window (real parts) and chip (imaginary parts; its bytes were sent toward L2 with the
-        // window) into the tile, zeros around them; the chip's FP64 sum and sum of squares as it
-        // goes (every product of two floats is exact in FP64), per warp
-        float cr[JN][IN];
-#pragma unroll
-        for (int j = 0; j < JN; ++j)
-#pragma unroll
-            for (int i = 0; i < IN; ++i) {
-                const int y = warp + kSpecWarps * j, x = lane + 32 * i;
-                cr[j][i] = y < R && x < R ? __ldg(chip + y * cs + x) : 0.0f;
-            }
+        // window) into the tile, zeros around them.  Raster windows: the chip goes in zero-mean
+        // and |r'|^2 is summed as spec_kernel sums it, the window's sums are taken on the way.
+        // Refined tiles: the chip goes in as it is, its FP64 sum and sum of squares taken on the
+        // way (every product of two floats is exact in FP64), and the first transform pass takes
+        // its mean off.
+        if constexpr (!RASTER) load_chip();
+        const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
         double c1 = 0.0, c2 = 0.0;
+        float sw = 0.0f, sw2 = 0.0f, sc2 = 0.0f;
         auto put = [&](int j, int i, float t) {
             const int y = warp + kSpecWarps * j, x = lane + 32 * i;
             if (y < N && x < N) {
-                const float c = cr[j][i];
-                c1 += (double)c;
-                c2 = fma((double)c, (double)c, c2);
+                float c = cr[j][i];
+                if constexpr (RASTER) {
+                    if (y < R && x < R) {
+                        c = (c - mc_hi) - mc_lo;
+                        sc2 = fmaf(c, c, sc2);
+                    }
+                    if (y < W && x < W) {
+                        const float d = t - pk;
+                        sw += d;
+                        sw2 = fmaf(d, d, sw2);
+                    }
+                } else {
+                    c1 += (double)c;
+                    c2 = fma((double)c, (double)c, c2);
+                }
                 Z[y * RS + x] = make_float2(t, c);
             }
         };
@@ -832,30 +855,50 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
 #pragma unroll
                     for (int i = 0; i < IN; ++i) put(j0 + q, i, v[q][i]);
         }
-        c1 = warp_sum(c1);
-        c2 = warp_sum(c2);
-        if (lane == 0) {
-            red[2 * warp] = c1;
-            red[2 * warp + 1] = c2;
-        }
-        __syncthreads();
-        double s1 = 0.0, s2 = 0.0;
-        for (int w = 0; w < kSpecWarps; ++w) {
-            s1 += red[2 * w];
-            s2 += red[2 * w + 1];
-        }
-        // |r'|^2 = S2 - S1^2 / R^2 of the zero-mean chip; a chip flat to within its own rounding
-        // (a constant: its zero-mean values are exactly 0) gets 0, as spec_kernel's sum of the
-        // squared zero-mean values gives it
-        const double mean_c = s1 / cells_c;
-        const double ss = s2 - s1 * mean_c;
-        const float inv_sigma = ss > 1e-14 * s2 ? (float)(1.0 / sqrt(ss)) : 0.0f;
-        const float mc_hi = (float)mean_c, mc_lo = (float)(mean_c - (double)mc_hi);
-        // the window mean and the chip's mean come off as the first transform pass reads the tile
+        double ss;
         fft::Centre centre{sx, W};
-        centre.ci_hi = mc_hi;
-        centre.ci_lo = mc_lo;
-        centre.ci = R;
+        if constexpr (RASTER) {
+            const double d0 = warp_sum((double)sc2), d1 = warp_sum((double)sw), d2 = warp_sum((double)sw2);
+            if (lane == 0) {
+                red[3 * warp] = d0;
+                red[3 * warp + 1] = d1;
+                red[3 * warp + 2] = d2;
+            }
+            __syncthreads();
+            ss = 0.0;
+            for (int w = 0; w < kSpecWarps; ++w) {
+                ss += red[3 * w];
+                wsum[0] += red[3 * w + 1];
+                wsum[1] += red[3 * w + 2];
+            }
+            mean_w = (double)pk + wsum[0] / cells_w;
+            st = fmax(wsum[1] - wsum[0] * wsum[0] / cells_w, 0.0) + 1e-5 * wsum[1];
+            centre.sx = (float)mean_w;
+        } else {
+            c1 = warp_sum(c1);
+            c2 = warp_sum(c2);
+            if (lane == 0) {
+                red[2 * warp] = c1;
+                red[2 * warp + 1] = c2;
+            }
+            __syncthreads();
+            double s1 = 0.0, s2 = 0.0;
+            for (int w = 0; w < kSpecWarps; ++w) {
+                s1 += red[2 * w];
+                s2 += red[2 * w + 1];
+            }
+            // |r'|^2 = S2 - S1^2 / R^2 of the zero-mean chip; a chip flat to within its own
+            // rounding (a constant: its zero-mean values are exactly 0) gets 0, as the sum of the
+            // squared zero-mean values gives it
+            mean_c = s1 / cells_c;
+            ss = s2 - s1 * mean_c;
+            if (!(ss > 1e-14 * s2)) ss = 0.0;
+            const float hi = (float)mean_c;
+            centre.ci_hi = hi;
+            centre.ci_lo = (float)(mean_c - (double)hi);
+            centre.ci = R;
+        }
+        const float inv_sigma = ss > 0.0 ? (float)(1.0 / sqrt(ss)) : 0.0f;
 
         const float scale = (float)(1.0 / (4.0 * (double)N * (double)N));
         const float ebox = kSpecErr * (float)sqrt(st);
@@ -877,9 +920,7 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
                 }
             },
             [&]() {
-                // the given statistics have landed; the staged bytes are free from here on: the
-                // next pair's window comes in
-                if constexpr (RASTER) cp_async_wait_all();
+                // the staged bytes are free from here on: the next pair's window comes in
                 fence_async_smem();
                 __syncthreads();
                 if (bn < pairs) {
@@ -943,16 +984,54 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
     float2* Y = X + N * RSN;                     // columns upsampled: F x N
     float2* twn = Y + F * RSY;
     float2* twf = twn + N;
-    for (int y = warp; y < N; y += kWarps)
-        for (int x = lane; x < N; x += 32) cp_async8_g(X + y * RSN + x, src + y * stride + x);
     for (int k = tid; k < N; k += kThreads) twn[k] = __ldg(twn_g + k);
     for (int k = tid; k < F; k += kThreads) twf[k] = __ldg(twf_g + k);
-    cp_async_wait_all();
-    __syncthreads();
-    // the upsampled-columns buffer is free until the columns are written: the deramp's scratch
-    if (DERAMP) deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
-    // the tile's mean comes off as the rows are read and back on with the amplitudes
-    const float2 mu = tile_mean<false, false>(X, RSN, N, 0.0f, 0.0f, reinterpret_cast<double*>(Y));
+    float2 mu;
+    if constexpr (DERAMP) {
+        for (int y = warp; y < N; y += kWarps)
+            for (int x = lane; x < N; x += 32) cp_async8_g(X + y * RSN + x, src + y * stride + x);
+        cp_async_wait_all();
+        __syncthreads();
+        // the upsampled-columns buffer is free until the columns are written: the deramp's scratch
+        deramp_tile(X, RSN, N, reinterpret_cast<double*>(Y));
+        // the tile's mean comes off as the rows are read and back on with the amplitudes
+        mu = tile_mean<false, false>(X, RSN, N, 0.0f, 0.0f, reinterpret_cast<double*>(Y));
+    } else {
+        // the tile through registers, its sum taken on the way (tile_mean's order: FP32 sums per
+        // thread over samples tid, tid + kThreads, ..., FP64 across the block); the mean comes
+        // off as the rows are read and back on with the amplitudes
+        constexpr int KT = (N * N + kThreads - 1) / kThreads;
+        float2 v[KT];
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            const int k = tid + q * kThreads;
+            v[q] = k < N * N ? __ldg(src + (k / N) * stride + k % N) : make_float2(0.0f, 0.0f);
+        }
+        float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            const int k = tid + q * kThreads;
+            if (k < N * N) {
+                X[(k / N) * RSN + k % N] = v[q];
+                sx += v[q].x;
+                sy += v[q].y;
+            }
+        }
+        double* red = reinterpret_cast<double*>(Y);
+        const double a = warp_sum((double)sx), b = warp_sum((double)sy);
+        if (lane == 0) {
+            red[2 * warp] = a;
+            red[2 * warp + 1] = b;
+        }
+        __syncthreads();
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            ta += red[2 * w];
+            tb += red[2 * w + 1];
+        }
+        const double cells = (double)N * (double)N;
+        mu = make_float2((float)(ta / cells), (float)(tb / cells));
+    }
     // rows: forward N
     for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a_minus<N1, N2>(X + (t % N) * RSN, 1, t / N, twn, mu);
     __syncthreads();
@@ -1815,7 +1894,7 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
                                const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
-                               const CUtensorMap* cmap)
+                               const CUtensorMap* cmap, const CUtensorMap* imap)
 {
     if (pairs <= 0) return cudaSuccess;
     const unsigned blocks = (unsigned)std::min<long long>(pairs, std::max(1u, sms));
@@ -1823,10 +1902,10 @@ cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st,
     if (g.N == NN) {                                                                                    \
         if (wmap)                                                                                       \
             spec_staged_kernel<A, B, true><<<blocks, kSpecThreads, g.smem_staged, st>>>(                      \
-                src, pair0, pairs, valid, g, inv, tw, out, errs, *wmap, *cmap);                             \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, *wmap, *cmap, *imap);                      \
         else                                                                                            \
             spec_staged_kernel<A, B, false><<<blocks, kSpecThreads, g.smem_staged, st>>>(                     \
-                src, pair0, pairs, valid, g, inv, tw, out, errs, CUtensorMap{}, CUtensorMap{});             \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, CUtensorMap{}, CUtensorMap{}, CUtensorMap{}); \
         return cudaGetLastError();                                                                      \
     }
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)
