@@ -361,6 +361,145 @@ HD void inv_a_store(const float2* base, int es, int n2, const float2* tw, Store 
     for (int n1 = 0; n1 < N1; ++n1) store(N2 * n1 + n2, a[n1]);
 }
 
+// Two tasks of one step at a time, their loads issued before either's arithmetic and their
+// stores after it (the tasks of a step touch disjoint elements): twice the independent work per
+// thread between two shared-memory round trips.
+template <int N1, int N2>
+HD void fwd_a_centred2(float2* ra, int ya, int n2a, float2* rb, int yb, int n2b, const float2* tw,
+                       const Centre& c)
+{
+    const int la = ya < c.wx ? c.wx : 0, lb = yb < c.wx ? c.wx : 0;
+    const int ia = ya < c.ci ? c.ci : 0, ib = yb < c.ci ? c.ci : 0;
+    float2 a[N1], b[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        a[n1] = ra[N2 * n1 + n2a];
+        b[n1] = rb[N2 * n1 + n2b];
+    }
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        const int na = N2 * n1 + n2a, nb = N2 * n1 + n2b;
+        if (na < la) a[n1].x -= c.sx;
+        if (na < ia) a[n1].y = (a[n1].y - c.ci_hi) - c.ci_lo;
+        if (nb < lb) b[n1].x -= c.sx;
+        if (nb < ib) b[n1].y = (b[n1].y - c.ci_hi) - c.ci_lo;
+    }
+    Dft<N1, -1>::run(a);
+    Dft<N1, -1>::run(b);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+        a[k1] = cmul(a[k1], tw[n2a * k1]);
+        b[k1] = cmul(b[k1], tw[n2b * k1]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+        ra[N2 * k1 + n2a] = a[k1];
+        rb[N2 * k1 + n2b] = b[k1];
+    }
+}
+
+template <int N1, int N2>
+HD void fwd_a2(float2* ba, int n2a, float2* bb, int n2b, int es, const float2* tw)
+{
+    float2 a[N1], b[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        a[n1] = ba[(N2 * n1 + n2a) * es];
+        b[n1] = bb[(N2 * n1 + n2b) * es];
+    }
+    Dft<N1, -1>::run(a);
+    Dft<N1, -1>::run(b);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+        a[k1] = cmul(a[k1], tw[n2a * k1]);
+        b[k1] = cmul(b[k1], tw[n2b * k1]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+        ba[(N2 * k1 + n2a) * es] = a[k1];
+        bb[(N2 * k1 + n2b) * es] = b[k1];
+    }
+}
+
+template <int N1, int N2, int S>
+HD void step_b2(float2* ba, int k1a, float2* bb, int k1b, int es)
+{
+    float2 a[N2], b[N2];
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+        a[j] = ba[(N2 * k1a + j) * es];
+        b[j] = bb[(N2 * k1b + j) * es];
+    }
+    Dft<N2, S>::run(a);
+    Dft<N2, S>::run(b);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+        ba[(N2 * k1a + j) * es] = a[j];
+        bb[(N2 * k1b + j) * es] = b[j];
+    }
+}
+
+template <int N1, int N2>
+HD void inv_a_lim2(float2* ba, int n2a, float2* bb, int n2b, int es, const float2* tw, int lim)
+{
+    float2 a[N1], b[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+        a[k1] = ba[(N2 * k1 + n2a) * es];
+        b[k1] = bb[(N2 * k1 + n2b) * es];
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+        a[k1] = cmulc(a[k1], tw[n2a * k1]);
+        b[k1] = cmulc(b[k1], tw[n2b * k1]);
+    }
+    Dft<N1, 1>::run(a);
+    Dft<N1, 1>::run(b);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+        if (N2 * n1 + n2a < lim) ba[(N2 * n1 + n2a) * es] = a[n1];
+        if (N2 * n1 + n2b < lim) bb[(N2 * n1 + n2b) * es] = b[n1];
+    }
+}
+
+// row_tasks two at a time: f2(ya, ja, yb, jb) for the tasks t and t + nt, f(y, j) for an odd
+// last one
+template <class F, class F2>
+HD void row_tasks2(int rows, int J, int tid, int nt, F f, F2 f2)
+{
+    const int dj = nt / rows, dy = nt - dj * rows;
+    auto step = [&](int& y, int& j) {
+        y += dy;
+        j += dj;
+        if (y >= rows) {
+            y -= rows;
+            ++j;
+        }
+    };
+    int j = tid / rows, y = tid - j * rows;
+    while (j < J) {
+        int yb = y, jb = j;
+        step(yb, jb);
+        if (jb >= J) {
+            f(y, j);
+            break;
+        }
+        f2(y, j, yb, jb);
+        y = yb;
+        j = jb;
+        step(y, j);
+    }
+}
+
+// tasks t = tid, tid + nt, ... below n, two at a time: f2(ta, tb), and f(t) for an odd last one
+template <class F, class F2>
+HD void tasks2(int n, int tid, int nt, F f, F2 f2)
+{
+    int t = tid;
+    for (; t + nt < n; t += 2 * nt) f2(t, t + nt);
+    if (t < n) f(t);
+}
+
 // position of frequency k in the permuted spectrum, and the frequency at position p
 template <int N1, int N2>
 HD int pos_of(int k) { return N2 * (k % N1) + k / N1; }
@@ -535,22 +674,38 @@ struct NoHook {
     HD void operator()() const {}
 };
 
-template <int N1, int N2, class Sync, class Store, class Hook = NoHook>
+// PAIR: 2 runs every pass two tasks at a time, 1 only the passes of N1-point steps (fewer
+// registers), 0 none
+template <int N1, int N2, int PAIR = 0, class Sync, class Store, class Hook = NoHook>
 HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float2* tw,
                        const int* neg, const int* half, const Centre& centre, int tid, int nt,
                        Sync sync, Store store, Hook cols_done = Hook{})
 {
     constexpr int N = N1 * N2;
     // forward along rows (centring the tile on the way in): lanes take consecutive rows
-    row_tasks(rows_in, N2, tid, nt, [&](int y, int n2) { fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre); });
+    if constexpr (PAIR >= 1)
+        row_tasks2(
+            rows_in, N2, tid, nt, [&](int y, int n2) { fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre); },
+            [&](int ya, int na, int yb, int nb) {
+                fwd_a_centred2<N1, N2>(Z + ya * RS, ya, na, Z + yb * RS, yb, nb, tw, centre);
+            });
+    else
+        row_tasks(rows_in, N2, tid, nt, [&](int y, int n2) { fwd_a_centred<N1, N2>(Z + y * RS, y, n2, tw, centre); });
     sync();
-    row_tasks(rows_in, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, -1>(Z + y * RS, 1, k1); });
+    if constexpr (PAIR >= 2)
+        row_tasks2(
+            rows_in, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, -1>(Z + y * RS, 1, k1); },
+            [&](int ya, int ka, int yb, int kb) { step_b2<N1, N2, -1>(Z + ya * RS, ka, Z + yb * RS, kb, 1); });
+    else
+        row_tasks(rows_in, N1, tid, nt, [&](int y, int k1) { step_b<N1, N2, -1>(Z + y * RS, 1, k1); });
     sync();
     // forward along columns: lanes take consecutive columns
-    for (int t = tid; t < N * N2; t += nt) {
-        const int x = t % N, n2 = t / N;
-        fwd_a<N1, N2>(Z + x, RS, n2, tw);
-    }
+    if constexpr (PAIR >= 1)
+        tasks2(
+            N * N2, tid, nt, [&](int t) { fwd_a<N1, N2>(Z + t % N, RS, t / N, tw); },
+            [&](int ta, int tb) { fwd_a2<N1, N2>(Z + ta % N, ta / N, Z + tb % N, tb / N, RS, tw); });
+    else
+        for (int t = tid; t < N * N2; t += nt) fwd_a<N1, N2>(Z + t % N, RS, t / N, tw);
     sync();
     // the columns' forward step B, the correlation spectrum and the inverse's step B on the
     // columns of the Hermitian half, one task per pair of column groups
@@ -566,10 +721,14 @@ HD void correlate_tile(float2* Z, int RS, int rows_in, int rows_out, const float
     }
     sync();
     // (only the placement rows are read from here on)
-    for (int t = tid; t < NH * N2; t += nt) {
-        const int c = t % NH, n2 = t / NH;
-        inv_a_lim<N1, N2>(Z + half[c], RS, n2, tw, rows_out);
-    }
+    if constexpr (PAIR >= 1)
+        tasks2(
+            NH * N2, tid, nt, [&](int t) { inv_a_lim<N1, N2>(Z + half[t % NH], RS, t / NH, tw, rows_out); },
+            [&](int ta, int tb) {
+                inv_a_lim2<N1, N2>(Z + half[ta % NH], ta / NH, Z + half[tb % NH], tb / NH, RS, tw, rows_out);
+            });
+    else
+        for (int t = tid; t < NH * N2; t += nt) inv_a_lim<N1, N2>(Z + half[t % NH], RS, t / NH, tw, rows_out);
     sync();
     cols_done();
     const int np = (rows_out + 1) / 2;

@@ -905,7 +905,7 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         float bv = -INFINITY;
         int bi = INT_MAX;
         int flagged = 0;
-        fft::correlate_tile<N1, N2>(
+        fft::correlate_tile<N1, N2, RASTER ? 2 : 0>(
             Z, RS, W, C, tw, neg, half, centre, tid, kSpecThreads, BlockSync{},
             [&](int u, int v, float2 val) {
                 if (v < C) {

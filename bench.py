@@ -412,9 +412,9 @@ def run_b200(args):
             }
         work["zoom"] = ("tensor", 2.0 * (Z * Cf * Cf + Z * Z * Cf))
         names = {
-            "coarse_correlation": {"tensor": "tc_coarse_kernel", "spectral": "spec_kernel (coarse)"}
+            "coarse_correlation": {"tensor": "tc_coarse_kernel", "spectral": "spec_staged_kernel (coarse)"}
             .get(worker.form, "coarse_kernel"),
-            "fine_correlation": {"tensor": "tc_fine_kernel", "spectral": "spec_kernel (fine)"}
+            "fine_correlation": {"tensor": "tc_fine_kernel", "spectral": "spec_staged_kernel (fine)"}
             .get(worker.form, "fine_kernel"),
             "refinement": {"spectral": "spec_refine_kernel (chip + window)"}.get(worker.form, "refine_kernel"),
             "coarse_statistics": {"spectral": "detect_kernel + box_vsum_kernel + box_inv_kernel (per raster)"}
@@ -454,11 +454,13 @@ def run_b200(args):
         if worker.form == "spectral":
             # the spectral kernels are bound by instruction issue, not by memory: their FFT
             # arithmetic (5 N log2 N flops per complex N-point transform) against the measured FP32
-            # FMA peak
+            # FMA peak; a correlation runs W forward row transforms, N forward column transforms,
+            # N / 2 + 1 inverse column transforms (the Hermitian half) and (C + 1) / 2 inverse row
+            # transforms (two placement rows each)
             nc, nf = spec_length(W), spec_length(Wf)
             fft = {
-                "coarse_correlation": (W + 2 * nc + C) * fft_flops(nc),
-                "fine_correlation": (Wf + 2 * nf + Cf) * fft_flops(nf),
+                "coarse_correlation": (W + nc + nc // 2 + 1 + (C + 1) // 2) * fft_flops(nc),
+                "fine_correlation": (Wf + nf + nf // 2 + 1 + (Cf + 1) // 2) * fft_flops(nf),
                 "refinement": sum(n * fft_flops(n) + n * fft_flops(f * n) + f * n * fft_flops(n)
                                   + f * n * fft_flops(f * n) for n in (R, E)),
             }
