@@ -302,7 +302,7 @@ bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
     g.off_inv = (int)off;
     off = up(off + (long)C * C * 4, 16);
     g.off_gam = (int)off;  // the surface; before the last step, the statistics' partial sums
-    const long limit = 227L * 1024 - 16;
+    const long limit = 227L * 1024 - 32;
     g.nseg = std::max(1, kSpecThreads / W);
     while (g.nseg > 1 && off + 32L * g.nseg * W > limit) --g.nseg;
     off = up(off + std::max<long>((long)C * C * 4, 32L * g.nseg * W), 128);
@@ -311,8 +311,8 @@ bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
     g.off_inv_raw = dense ? 0 : (int)off;
     if (!dense) off = up(off + (long)C * g.inv_rs * 4, 16);
     g.off_bar = (int)off;
-    off += 16;
-    g.smem_staged = off <= limit + 16 ? (int)off : 0;
+    off += 32;  // the copy's mbarrier, the wait-failure flag, the failure-detection test's mbarrier
+    g.smem_staged = off <= 227L * 1024 ? (int)off : 0;
     return g.smem_staged > 0;
 }
 
@@ -1054,7 +1054,7 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
             if (coarse_st)
                 CK(h, launch_spec_staged(h->spc_st, (unsigned)h->sms, st, cs, c0, n, src.ref_off, r.inv_c,
                                          reinterpret_cast<const float2*>(h->d_tw_c), co, h->d_tc_err,
-                                         &wmap, &cmap, &imap),
+                                         &wmap, &cmap, &imap, h->inject_timeouts > 0 ? 1 : 0),
                    "launching the staged coarse correlation");
             else
                 CK(h, launch_spec(h->spc, n, st, cs, c0, n, src.ref_off, r.inv_c,
@@ -1102,7 +1102,7 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                 CK(h, launch_spec_staged(h->spf_st, (unsigned)h->sms, st, fs, c0, n, src.ref_off,
                                          InvSource{nullptr, nullptr, 0},
                                          reinterpret_cast<const float2*>(h->d_tw_f), fo, h->d_tc_err,
-                                         nullptr, nullptr, nullptr),
+                                         nullptr, nullptr, nullptr, h->inject_timeouts > 0 ? 1 : 0),
                    "launching the staged fine correlation");
             else
                 CK(h, launch_spec(h->spf, n, st, fs, c0, n, src.ref_off, InvSource{nullptr, nullptr, 0},

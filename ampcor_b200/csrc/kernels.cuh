@@ -331,10 +331,10 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 // counted in errs.  Refined tiles: wmap and cmap null, no statistics given.  Raster windows:
 // wmap, cmap and imap 2-D maps of the secondary and reference amplitude rasters and of the
 // secondary's box statistics (inv) with boxes of stage_rs x W, (R + 6 & ~3) x R and inv_rs x C
-// floats.
+// floats.  stall: the failure-detection test's wait on a barrier that nothing completes.
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
                                const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
-                               const CUtensorMap* cmap, const CUtensorMap* imap);
+                               const CUtensorMap* cmap, const CUtensorMap* imap, int stall);
 
 }  // namespace ampcor_b200

@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kSpecThreads, 1)
 spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long long* valid, SpecGeom g,
                    InvSource inv, const float2* tw_g, SpecOut out, unsigned int* errs,
                    const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap cmap,
-                   const __grid_constant__ CUtensorMap imap)
+                   const __grid_constant__ CUtensorMap imap, int stall)
 {
     extern __shared__ __align__(16) unsigned char ssm[];
     constexpr int N = N1 * N2;
@@ -660,9 +660,17 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
     if (tid == 0) {
         s_err = 0;
         mbar_init(bar, 1);
+        mbar_init(bar + 2, 1);  // completed by nothing: the wait of a failure-detection test
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // a failure-detection test: before any copy is issued, every thread waits on a barrier that
+    // nothing completes; the bounded wait runs out, sets the error flag, and the CTA skips its
+    // pairs and reports the time-out like any other expired wait
+    if (stall) {
+        mbar_wait(bar + 2, 0u, &s_err, kStallCycles);
+        __syncthreads();
+    }
     // warp 0: the window rows of chunk pair b into the staging bytes, the chip rows toward L2; a
     // pair without tiles (its offsets are -1) copies nothing and completes the phase at once
     auto issue = [&](long long b) {
@@ -691,17 +699,22 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
             }
         }
     };
-    if (warp == 0 && blockIdx.x < pairs) issue(blockIdx.x);
+    const bool run = !stall || !s_err;
+    if (warp == 0 && blockIdx.x < pairs && run) issue(blockIdx.x);
     uint32_t parity = 0;
-    bool inflight = blockIdx.x < pairs;
-    for (long long b = blockIdx.x; b < pairs; b += gridDim.x) {
+    bool inflight = blockIdx.x < pairs && run;
+    long long b_left = blockIdx.x;  // (raster windows) the first pair left without a result
+    for (long long b = blockIdx.x; b < pairs && run; b += gridDim.x) {
         const long long p = pair0 + b;
         const long long bn = b + gridDim.x;
         const bool ok = valid[p] >= 0;
         const float* chip = spec_chip(src, pair0, b);
         const float* win = spec_win(src, pair0, b);
         const bool landed = mbar_wait(bar, parity, &s_err);
-        if (__syncthreads_or(!landed)) break;
+        if (__syncthreads_or(!landed)) {
+            if constexpr (RASTER) b_left = b;
+            break;
+        }
         parity ^= 1u;
         inflight = false;
         if (!ok) {
@@ -936,10 +949,16 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
         if (tid == 0) spec_result(out, p, R, W, C, bv, bi);
     }
     if (s_err) {
-        // a wait ran out: count it once per CTA and let the copy in flight land before the shared
-        // memory is given up
+        // a wait ran out: count it once per CTA, give the pairs left a coarse result whose
+        // refinement corners stay inside their windows, and let the copy in flight land before
+        // the shared memory is given up
         if (tid == 0) {
             atomicAdd(errs, 1u);
+            if constexpr (RASTER)
+                for (long long q = b_left; q < pairs; q += gridDim.x) {
+                    out.coarse[pair0 + q] = CoarseOut{-1, -1, 0, 0};
+                    out.coarse_peak[pair0 + q] = NAN;
+                }
             if (inflight) {
                 const long long t0 = clock64();
                 while (!mbar_try(bar, parity) && clock64() - t0 < kSpinCycles) {
@@ -1894,7 +1913,7 @@ cudaError_t launch_spec(const SpecGeom& g, unsigned blocks, cudaStream_t st, Spe
 cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st, SpecSource src,
                                long long pair0, long long pairs, const long long* valid, InvSource inv,
                                const float2* tw, SpecOut out, unsigned int* errs, const CUtensorMap* wmap,
-                               const CUtensorMap* cmap, const CUtensorMap* imap)
+                               const CUtensorMap* cmap, const CUtensorMap* imap, int stall)
 {
     if (pairs <= 0) return cudaSuccess;
     const unsigned blocks = (unsigned)std::min<long long>(pairs, std::max(1u, sms));
@@ -1902,10 +1921,11 @@ cudaError_t launch_spec_staged(const SpecGeom& g, unsigned sms, cudaStream_t st,
     if (g.N == NN) {                                                                                    \
         if (wmap)                                                                                       \
             spec_staged_kernel<A, B, true><<<blocks, kSpecThreads, g.smem_staged, st>>>(                      \
-                src, pair0, pairs, valid, g, inv, tw, out, errs, *wmap, *cmap, *imap);                      \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, *wmap, *cmap, *imap, stall);               \
         else                                                                                            \
             spec_staged_kernel<A, B, false><<<blocks, kSpecThreads, g.smem_staged, st>>>(                     \
-                src, pair0, pairs, valid, g, inv, tw, out, errs, CUtensorMap{}, CUtensorMap{}, CUtensorMap{}); \
+                src, pair0, pairs, valid, g, inv, tw, out, errs, CUtensorMap{}, CUtensorMap{}, CUtensorMap{},  \
+                stall);                                                                             \
         return cudaGetLastError();                                                                      \
     }
     AMPCOR_SPEC_LENGTHS(AMPCOR_SPEC_CASE)

@@ -204,11 +204,12 @@ int ampcor_configure(ampcor_handle* handle, int form, uint64_t chunk);
 
 /* Failure-detection test hook (no reference counterpart; the reference has no bounded waits).
    The next `batches` batches of the worker (tensor-core or spectral form) make the first wait of
-   their tensor-core zoom on a barrier that nothing completes, bounded at about a millisecond:
-   every wait of the tensor-core kernels is bounded in time, and an expired wait stops the kernel
-   cleanly and is reported.  The zoom issues no work after it and writes no offsets for those
-   batches, and the ampcor_synchronize() that ends each of them returns AMPCOR_E_CUDA with a
-   time-out message; the worker stays usable.  0 switches it off. */
+   their tensor-core zoom, and of the staged spectral correlation kernels, on a barrier that
+   nothing completes, bounded at about a millisecond: every wait of those kernels is bounded in
+   time, and an expired wait stops the kernel cleanly and is reported.  The kernels issue no work
+   after it and write no offsets for those batches (a staged coarse stage leaves its pairs
+   refinement corners inside their windows), and the ampcor_synchronize() that ends each of them
+   returns AMPCOR_E_CUDA with a time-out message; the worker stays usable.  0 switches it off. */
 int ampcor_inject_timeout(ampcor_handle* handle, int batches);
 
 /* The number of pairs refined per chunk. */

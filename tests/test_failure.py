@@ -1,11 +1,12 @@
 """Failure detection without a GPU fault (needs a B200).
 
-Every wait of the tensor-core kernels is bounded in time; an expired wait sets an error flag, the
-kernel stops issuing work, lets the work it issued finish, frees its tensor memory and returns,
-and the host reports the time-out.  Here a wait is made to run out on purpose, on a barrier that
-nothing completes (ampcor_inject_timeout), before any tensor-core work is issued: the batch must
-report AMPCOR_E_CUDA with the time-out message and the same worker must then run the next batch
-to the same offsets as before.
+Every wait of the tensor-core kernels and of the staged spectral correlation kernels (one
+resident CTA per SM, windows brought in by the copy engine) is bounded in time; an expired wait
+sets an error flag, the kernel stops issuing work, lets the work it issued finish, frees its
+tensor memory and returns, and the host reports the time-out.  Here a wait is made to run out on
+purpose, on a barrier that nothing completes (ampcor_inject_timeout), before any copy or
+tensor-core work is issued: the batch must report AMPCOR_E_CUDA with the time-out message and the
+same worker must then run the next batch to the same offsets as before.
 """
 import numpy as np
 import pytest
