@@ -560,6 +560,7 @@ struct ampcor_handle {
     // multiprocessors
     SpecGeom spc_st{}, spf_st{};
     bool coarse_staged = false, fine_staged = false;
+    bool staged_on = false;  // the staged forms are allowed (AMPCOR_STAGED is not 0)
     int sms = 0;
     // tensor-core zoom (both the tensor-core and the spectral forms), when Zm fits
     bool zoom_tc = false;
@@ -1026,6 +1027,15 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
         raster_map(wmap, r.amp_tgt, src.tgt_count / src.tgt_stride, src.tgt_stride, h->spc_st.stage_rs, h->W) &&
         raster_map(cmap, r.amp_ref, src.ref_count / src.ref_stride, src.ref_stride, (h->R + 6) & ~3, h->R) &&
         raster_map(imap, r.inv_c.base, r.rows, src.tgt_stride, h->spc_st.inv_rs, h->C);
+    // the window refinement of a raster job in the staged form: its tiles come from the secondary
+    // raster (as floats, two a sample) through a tensor map
+    CUtensorMap rmap{};
+    int rs_smem = 0, rs_box = 0;
+    const bool refine_st =
+        h->staged_on && h->refine_fft && !h->refine_strips && !(h->prm.flags & AMPCOR_FLAG_DERAMP) &&
+        src.tgt_lines > 0 && src.tgt_stride > 0 && spec_refine_staged_supported(h->E, h->f, rs_smem, rs_box) &&
+        raster_map(rmap, reinterpret_cast<const float*>(src.tgt_base), src.tgt_count / src.tgt_stride,
+                   2 * src.tgt_stride, rs_box, h->E);
     for (long long c0 = p0; c0 < p1; c0 += (long long)h->chunk) {
         const unsigned n = (unsigned)std::min<long long>((long long)h->chunk, p1 - c0);
         cudaEvent_t b = mark(h, st);
@@ -1069,11 +1079,18 @@ int spec_pairs(ampcor_handle* h, const PairSource& src, const SpecRasters& r, lo
                                      n, src.ref_off, tw, tw + h->R, h->d_refined, h->refined_stride, 0,
                                      (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy, h->refine_strips),
                "launching the chip refinement");
-            CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
-                                     c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
-                                     h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf,
-                                     (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy, h->refine_strips),
-               "launching the window refinement");
+            if (refine_st)
+                CK(h, launch_spec_refine_staged(h->E, (unsigned)h->sms, st, &rmap, src.tgt_off, src.tgt_stride,
+                                                h->d_coarse, c0, n, src.ref_off, tw + h->R + h->Rf,
+                                                tw + h->R + h->Rf + h->E, h->d_refined, h->refined_stride,
+                                                (long long)h->Rf * h->Rf, h->d_tc_err),
+                   "launching the staged window refinement");
+            else
+                CK(h, launch_spec_refine(h->E, n, st, src.tgt_base, src.tgt_off, src.tgt_stride, h->d_coarse,
+                                         c0, n, src.ref_off, tw + h->R + h->Rf, tw + h->R + h->Rf + h->E,
+                                         h->d_refined, h->refined_stride, (long long)h->Rf * h->Rf,
+                                         (h->prm.flags & AMPCOR_FLAG_DERAMP) ? 1 : 0, h->d_upy, h->refine_strips),
+                   "launching the window refinement");
         } else {
             refine_kernel<<<n, kThreads, h->refine_smem, st>>>(src, c0, n, h->d_coarse, h->ic, h->iw,
                                                                h->d_chip_taps, h->d_win_taps,
@@ -1235,6 +1252,7 @@ int ampcor_create(const ampcor_params* p, ampcor_handle** out)
         // pair are dense rows of one buffer, staged whole when its rows are 16-byte multiples
         const char* stg = std::getenv("AMPCOR_STAGED");
         const bool staged_on = !(stg && std::strcmp(stg, "0") == 0);
+        h->staged_on = staged_on;
         h->coarse_staged = staged_on && direct_c && plan_spec_staged(h->R, h->W, false, h->spc_st);
         h->fine_staged = staged_on && direct_f &&
                          plan_spec_staged(h->Rf, h->Wf, h->Rf % 2 == 0 && h->Wf % 2 == 0, h->spf_st) &&

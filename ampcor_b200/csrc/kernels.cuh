@@ -300,6 +300,16 @@ bool spec_refine_supported(int n, int f, int& smem);
 // (ybuf, blocks of them): tiles too large for one CTA's shared memory (N in 96 .. 160, f = 2), and
 // with `strips` the shorter compiled lengths too (less shared memory, more CTAs per SM)
 bool spec_refine_big_supported(int n, int f, int& smem);
+// refinement of raster windows by the staged kernel (one resident CTA per SM, the next tile copied
+// in by the copy engine): whether compiled for N x N tiles and factor f, its shared memory and the
+// width (floats) of the tensor map's box; tmap maps the secondary raster as floats (2 per sample)
+// with boxes of box_x x N floats
+bool spec_refine_staged_supported(int n, int f, int& smem, int& box_x);
+cudaError_t launch_spec_refine_staged(int n, unsigned sms, cudaStream_t st, const CUtensorMap* tmap,
+                                      const long long* off, long long stride, const CoarseOut* coarse,
+                                      long long pair0, long long pairs, const long long* valid,
+                                      const float2* twn, const float2* twf, float* refined,
+                                      long long refined_stride, long long out_off, unsigned int* errs);
 cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const float2* base,
                                const long long* off, long long stride, const CoarseOut* coarse,
                                long long pair0, long long pairs, const long long* valid,

@@ -989,7 +989,17 @@ struct UpsampleGeom {
     static constexpr int CB = CBX < 32 ? CBX : 32;
     static constexpr int smem = (N * RSN + F * RSY + N + F) * 8;
     static_assert(CB >= 1, "the row block must fit in the tile's space");
+    // staged form (spec_refine_staged_kernel): the tile as copied from the raster, N rows of SWS
+    // floats (2 N + 2 from the 16-byte boundary at or before its first sample), then the copy's
+    // mbarrier and the CTA's wait-failure flag
+    static constexpr int SWS = (2 * N + 5) & ~3;
+    static constexpr int off_stage = (smem + 127) / 128 * 128;
+    static constexpr int off_bar = off_stage + N * SWS * 4;
+    static constexpr int smem_staged = off_bar + 16;
 };
+
+template <int N1, int N2, int F1, int F2>
+__device__ void upsample_core(unsigned char* sm, float2 mu, float* __restrict__ out);
 
 template <int N1, int N2, int F1, int F2, bool DERAMP>
 __device__ void fft_upsample(const float2* __restrict__ src, long long stride, unsigned char* sm,
@@ -1051,6 +1061,21 @@ __device__ void fft_upsample(const float2* __restrict__ src, long long stride, u
         const double cells = (double)N * (double)N;
         mu = make_float2((float)(ta / cells), (float)(tb / cells));
     }
+    upsample_core<N1, N2, F1, F2>(sm, mu, out);
+}
+
+// the transforms of fft_upsample and the amplitudes out, from the tile in place (X) with its mean
+// mu and the twiddles in shared memory
+template <int N1, int N2, int F1, int F2>
+__device__ void upsample_core(unsigned char* sm, float2 mu, float* __restrict__ out)
+{
+    using G = UpsampleGeom<N1, N2, F1, F2>;
+    constexpr int N = G::N, F = G::F, RSN = G::RSN, RSY = G::RSY, RSB = G::RSB, CB = G::CB;
+    const int tid = threadIdx.x;
+    float2* X = reinterpret_cast<float2*>(sm);
+    float2* Y = X + N * RSN;
+    const float2* twn = Y + F * RSY;
+    const float2* twf = twn + N;
     // rows: forward N
     for (int t = tid; t < N * N2; t += kThreads) fft::fwd_a_minus<N1, N2>(X + (t % N) * RSN, 1, t / N, twn, mu);
     __syncthreads();
@@ -1112,6 +1137,135 @@ spec_refine_kernel(const float2* base, const long long* off, long long stride,
     }
     fft_upsample<N1, N2, F1, F2, DERAMP>(
         src, stride, rsm, twn, twf, refined + (long long)blockIdx.x * refined_stride + out_off);
+}
+
+// Refinement of the windows of a raster job, staged: one resident CTA per SM walks the pairs of
+// the chunk, and the copy engine brings the next pair's tile (the box of the secondary raster,
+// as floats, at the nudged corner of its coarse result) into a buffer of its own while this
+// pair's transforms run.  The tile goes from that buffer into place with its sum taken in
+// fft_upsample's order, so the amplitudes are fft_upsample's bit for bit.  Every wait is
+// bounded; one that runs out is counted in errs, the CTA lets its copy land (bounded) and returns.
+template <int N1, int N2, int F1, int F2>
+__global__ void __launch_bounds__(kThreads, 1)
+spec_refine_staged_kernel(const __grid_constant__ CUtensorMap tmap, const long long* off, long long stride,
+                          const CoarseOut* coarse, long long pair0, long long pairs, const long long* valid,
+                          const float2* twn_g, const float2* twf_g, float* refined, long long refined_stride,
+                          long long out_off, unsigned int* errs)
+{
+    extern __shared__ __align__(128) unsigned char rsm[];
+    using G = UpsampleGeom<N1, N2, F1, F2>;
+    constexpr int N = G::N, F = G::F, RSN = G::RSN, RSY = G::RSY, SWS = G::SWS;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float2* X = reinterpret_cast<float2*>(rsm);
+    float2* Y = X + N * RSN;
+    float2* twn = Y + F * RSY;
+    float2* twf = twn + N;
+    float* stage = reinterpret_cast<float*>(rsm + G::off_stage);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(rsm + G::off_bar);
+    int& s_err = *reinterpret_cast<int*>(rsm + G::off_bar + 8);
+    for (int k = tid; k < N; k += kThreads) twn[k] = __ldg(twn_g + k);
+    for (int k = tid; k < F; k += kThreads) twf[k] = __ldg(twf_g + k);
+    if (tid == 0) {
+        s_err = 0;
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // first sample of chunk pair b's tile: line y, sample x of the raster
+    auto corner = [&](long long b, int& x, int& y) {
+        const long long p = pair0 + b;
+        const CoarseOut co = coarse[p];
+        const long long o = off[p] + co.top * stride + co.left;
+        const long long yy = o / stride;
+        y = (int)yy;
+        x = (int)(o - yy * stride);
+    };
+    // thread 0: chunk pair b's tile into the staging buffer; a pair without tiles copies nothing
+    auto issue = [&](long long b) {
+        if (valid[pair0 + b] < 0) {
+            mbar_arrive(bar);
+            return;
+        }
+        int x, y;
+        corner(b, x, y);
+        mbar_expect_tx(bar, (unsigned)(N * SWS * 4));
+        tensor_to_smem(stage, &tmap, (2 * x) & ~3, y, bar);
+    };
+    if (tid == 0 && blockIdx.x < pairs) issue(blockIdx.x);
+    uint32_t parity = 0;
+    bool inflight = blockIdx.x < pairs;
+    for (long long b = blockIdx.x; b < pairs; b += gridDim.x) {
+        const long long p = pair0 + b;
+        const long long bn = b + gridDim.x;
+        const bool ok = valid[p] >= 0;
+        int of = 0;
+        if (ok) {
+            int x, y;
+            corner(b, x, y);
+            of = (2 * x) & 3;
+        }
+        const bool landed = mbar_wait(bar, parity, &s_err);
+        if (__syncthreads_or(!landed)) break;
+        parity ^= 1u;
+        inflight = false;
+        if (!ok) {
+            if (bn < pairs) {
+                fence_async_smem();
+                __syncthreads();
+                if (tid == 0) issue(bn);
+                inflight = true;
+            }
+            continue;
+        }
+        // the tile into place, its sum taken on the way (fft_upsample's order)
+        constexpr int KT = (N * N + kThreads - 1) / kThreads;
+        float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            const int k = tid + q * kThreads;
+            if (k < N * N) {
+                const int y = k / N, x = k % N;
+                const float2 v = *reinterpret_cast<const float2*>(stage + y * SWS + of + 2 * x);
+                X[y * RSN + x] = v;
+                sx += v.x;
+                sy += v.y;
+            }
+        }
+        double* red = reinterpret_cast<double*>(Y);
+        const double a = warp_sum((double)sx), c = warp_sum((double)sy);
+        if (lane == 0) {
+            red[2 * warp] = a;
+            red[2 * warp + 1] = c;
+        }
+        // the staging buffer is read: the next pair's tile comes in while this one is transformed
+        fence_async_smem();
+        __syncthreads();
+        if (bn < pairs) {
+            if (tid == 0) issue(bn);
+            inflight = true;
+        }
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            ta += red[2 * w];
+            tb += red[2 * w + 1];
+        }
+        const double cells = (double)N * (double)N;
+        const float2 mu = make_float2((float)(ta / cells), (float)(tb / cells));
+        upsample_core<N1, N2, F1, F2>(rsm, mu, refined + b * refined_stride + out_off);
+    }
+    if (s_err) {
+        // a wait ran out: count it once per CTA and let the copy in flight land before the shared
+        // memory is given up
+        if (tid == 0) {
+            atomicAdd(errs, 1u);
+            if (inflight) {
+                const long long t0 = clock64();
+                while (!mbar_try(bar, parity) && clock64() - t0 < kSpinCycles) {
+                }
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // refinement (N, F = 2 N) pairs that are compiled: N, N1, N2, F1, F2
@@ -1797,6 +1951,40 @@ cudaError_t launch_spec_refine(int n, unsigned blocks, cudaStream_t st, const fl
     return cudaErrorInvalidValue;
 }
 
+bool spec_refine_staged_supported(int n, int f, int& smem, int& box_x)
+{
+    smem = box_x = 0;
+    if (f != 2) return false;
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                        \
+    if (n == NN) {                                                \
+        smem = UpsampleGeom<A, B, C, D>::smem_staged;             \
+        box_x = UpsampleGeom<A, B, C, D>::SWS;                    \
+        return smem <= 227 * 1024 && box_x <= 256;                \
+    }
+    AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    return false;
+}
+
+cudaError_t launch_spec_refine_staged(int n, unsigned sms, cudaStream_t st, const CUtensorMap* tmap,
+                                      const long long* off, long long stride, const CoarseOut* coarse,
+                                      long long pair0, long long pairs, const long long* valid,
+                                      const float2* twn, const float2* twf, float* refined,
+                                      long long refined_stride, long long out_off, unsigned int* errs)
+{
+    if (pairs <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)std::min<long long>(pairs, std::max(1u, sms));
+#define AMPCOR_REFINE_CASE(NN, A, B, C, D)                                                           \
+    if (n == NN) {                                                                                   \
+        spec_refine_staged_kernel<A, B, C, D><<<blocks, kThreads, UpsampleGeom<A, B, C, D>::smem_staged, st>>>( \
+            *tmap, off, stride, coarse, pair0, pairs, valid, twn, twf, refined, refined_stride, out_off, errs); \
+        return cudaGetLastError();                                                                   \
+    }
+    AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
+#undef AMPCOR_REFINE_CASE
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t spec_set_smem_limits()
 {
     const int limit = 227 * 1024;
@@ -1805,7 +1993,9 @@ cudaError_t spec_set_smem_limits()
     if (e == cudaSuccess)                  \
         e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
     if (e == cudaSuccess)                  \
-        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+        e = cudaFuncSetAttribute(spec_refine_kernel<A, B, C, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit); \
+    if (e == cudaSuccess && UpsampleGeom<A, B, C, D>::smem_staged <= limit) \
+        e = cudaFuncSetAttribute(spec_refine_staged_kernel<A, B, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
     AMPCOR_REFINE_PAIRS(AMPCOR_REFINE_CASE)
 #undef AMPCOR_REFINE_CASE
 #define AMPCOR_SPEC_CASE(NN, A, B) \
