@@ -261,3 +261,20 @@ def test_forms_agree_with_plain(form):
     np.testing.assert_allclose(t["coarse"], p["coarse"], atol=SURF_ATOL, rtol=0)
     np.testing.assert_allclose(t["refined"], p["refined"], atol=SURF_ATOL, rtol=0)
     assert (t["offsets"] == p["offsets"]).all(axis=1).mean() > 0.98
+
+
+@pytest.mark.parametrize("shape,chip", [((500, 514), 32), ((590, 601), 32)])
+def test_copy_engine_edge_cases_parity(shape, chip):
+    """The staged kernels take their windows through the copy engine, which wants raster lines of
+    whole 16-byte units.  Lines of 514 samples (the amplitude raster's lines are not 16-byte
+    multiples, the complex raster's are: the coarse stage falls back to spec_kernel, the window
+    refinement stays staged) and of 601 samples (neither: both fall back) still give every pair
+    the FP64 oracle's offsets.  (Refined tiles are always whole 16-byte rows: tiles are multiples
+    of 8 samples.)"""
+    ref = synth.speckle(shape, 3)
+    tgt = (synth.fourier_shift(ref, 2.3, -1.6) + synth.noise(shape, 10.0, 4)).astype(np.complex64)
+    centres = synth.uniform_grid(shape, (6, 6))
+    ulhc, kept = synth._grid_pairs(shape, centres, chip, 8)
+    w = synth.Workload("edges", ref, tgt, ulhc, kept, chip, 8, 2, 4, 4, None)
+    gpu = run_device(w, form="spectral")
+    check_parity(w, w.ulhc, gpu, f"{shape} chip {chip}")
