@@ -265,7 +265,7 @@ bool plan_spec(int R, int W, SpecGeom& g, std::string& err)
 // are read, the others in pieces of kStagePieces row groups, none of which may reach the staged
 // rows of a later piece.  Rows whose samples may sit off 16-byte boundaries (`dense` false, or W
 // not a multiple of 4) get 3 + W floats rounded up to 16 bytes.
-constexpr int kStagePieces = 3;  // spec_staged_kernel's PJ
+constexpr int kStagePieces = 5;  // spec_staged_kernel's PJ
 
 bool plan_spec_staged(int R, int W, bool dense, SpecGeom& g)
 {

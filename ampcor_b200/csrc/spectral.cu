@@ -634,7 +634,7 @@ spec_staged_kernel(SpecSource src, long long pair0, long long pairs, const long 
     constexpr int N = N1 * N2;
     constexpr int RS = N + 1;
     constexpr int JN = (N + kSpecWarps - 1) / kSpecWarps, IN = (N + 31) / 32;
-    constexpr int PJ = 3;  // row groups of a piece read whole before it is written
+    constexpr int PJ = 5;  // row groups of a piece read whole before it is written
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int W = g.W, R = g.R, C = g.C, SW = g.stage_rs;
     float2* Z = reinterpret_cast<float2*>(ssm + g.off_z);
