@@ -1152,7 +1152,7 @@ spec_refine_staged_kernel(const __grid_constant__ CUtensorMap tmap, const long l
                           const float2* twn_g, const float2* twf_g, float* refined, long long refined_stride,
                           long long out_off, unsigned int* errs)
 {
-    extern __shared__ __align__(128) unsigned char rsm[];
+    extern __shared__ __align__(16) unsigned char rsm[];
     using G = UpsampleGeom<N1, N2, F1, F2>;
     constexpr int N = G::N, F = G::F, RSN = G::RSN, RSY = G::RSY, SWS = G::SWS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
